@@ -1,0 +1,663 @@
+// C ABI (include/ftlm_gpu.h): sector handles, H·v, Lanczos, quadrature, grand-canonical sweep.
+// Host orchestration only; every floating-point operation on sector vectors runs in the
+// kernels of hv.cu / lanczos.cu / quad.cu.  No exception crosses the ABI.
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "../../include/ftlm_gpu.h"
+#include "hv.cuh"
+#include "plan.hpp"
+
+using namespace ftlm_b200;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CU_TRY(expr)                                                                                     \
+  do {                                                                                                   \
+    cudaError_t e_ = (expr);                                                                             \
+    if (e_ != cudaSuccess)                                                                               \
+      return fail(e_ == cudaErrorMemoryAllocation ? FTLM_ERR_NOMEM : FTLM_ERR_CUDA,                      \
+                  std::string(#expr) + ": " + cudaGetErrorString(e_));                                   \
+  } while (0)
+
+template <class T>
+cudaError_t upload(const std::vector<T>& v, T** out, std::vector<void*>* owned) {
+  *out = nullptr;
+  const size_t bytes = std::max<size_t>(v.size(), 1) * sizeof(T);
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) return e;
+  owned->push_back(p);
+  if (!v.empty()) e = cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+  *out = static_cast<T*>(p);
+  return e;
+}
+
+// Device buffer that frees itself.
+struct DevBuf {
+  void* p = nullptr;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  cudaError_t alloc(size_t bytes) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    return cudaMalloc(&p, std::max<size_t>(bytes, 16));
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+// Reference start vector (src/lanczos.cpp:140-175): re, im from std::normal_distribution<double>
+// over std::mt19937(seed), normalised with a serial sum; falls back to e_0 when ||q|| < 1e-18.
+void reference_start(int64_t dim, unsigned seed, std::vector<std::complex<double>>* q) {
+  std::mt19937 rng(seed);
+  std::normal_distribution<double> gauss(0.0, 1.0);
+  q->resize(static_cast<size_t>(dim));
+  auto& v = *q;
+  for (int64_t i = 0; i < dim; ++i) {
+    const double re = gauss(rng);
+    const double im = gauss(rng);
+    v[static_cast<size_t>(i)] = {re, im};
+  }
+  double n0 = 0.0;
+  for (const auto& z : v) n0 += std::norm(z);
+  n0 = std::sqrt(n0);
+  if (n0 < 1e-18) {
+    std::fill(v.begin(), v.end(), std::complex<double>(0.0, 0.0));
+    v[0] = {1.0, 0.0};
+  } else {
+    const std::complex<double> sc(1.0 / n0, 0.0);
+    for (auto& z : v) z *= sc;
+  }
+}
+
+// Device Lanczos workspace.
+struct LanczosWs {
+  int64_t n = 0;
+  DevBuf q, qp, w, scratch;
+  cudaError_t ensure(int64_t dim) {
+    if (n == dim && q.p) return cudaSuccess;
+    n = dim;
+    cudaError_t e;
+    if ((e = q.alloc(dim * sizeof(double2))) != cudaSuccess) return e;
+    if ((e = qp.alloc(dim * sizeof(double2))) != cudaSuccess) return e;
+    if ((e = w.alloc(dim * sizeof(double2))) != cudaSuccess) return e;
+    return scratch.alloc(kScratchDoubles * sizeof(double));
+  }
+};
+
+// Generic Lanczos loop around an operator on device vectors; the recurrence of
+// src/lanczos.cpp:180-205 with alpha, ||w||^2 read back once per step for the breakdown test.
+template <class Apply>
+int run_lanczos(int64_t dim, Apply&& apply, LanczosWs& ws, int max_steps, unsigned seed, int start_mode,
+                cudaStream_t st, std::vector<double>* alpha, std::vector<double>* beta) {
+  alpha->clear();
+  beta->clear();
+  if (dim <= 0 || max_steps <= 0) return FTLM_OK;
+  CU_TRY(ws.ensure(dim));
+  double* scr = ws.scratch.as<double>();
+  if (start_mode == FTLM_START_PHILOX) {
+    CU_TRY(lz_philox_start(ws.q.as<double2>(), dim, seed, scr, st));
+    CU_TRY(lz_normalise_start(ws.q.as<double2>(), dim, scr, st));
+  } else if (start_mode == FTLM_START_REFERENCE) {
+    std::vector<std::complex<double>> h;
+    reference_start(dim, seed, &h);
+    CU_TRY(cudaMemcpyAsync(ws.q.p, h.data(), dim * sizeof(double2), cudaMemcpyHostToDevice, st));
+    CU_TRY(cudaStreamSynchronize(st));
+  } else {
+    return fail(FTLM_ERR_INVALID, "unknown start_mode");
+  }
+  double2* q = ws.q.as<double2>();
+  double2* qp = ws.qp.as<double2>();
+  double2* w = ws.w.as<double2>();
+  double bprev = 0.0;
+  double res[4];
+  for (int k = 0; k < max_steps; ++k) {
+    const int rc = apply(q, w, st);
+    if (rc != FTLM_OK) return rc;
+    CU_TRY(lz_dotc(q, w, dim, scr, st));
+    CU_TRY(lz_update(w, q, qp, bprev, k > 0, dim, scr, st));
+    // Next q into the old q_prev buffer (harmless if this step turns out to be the last).
+    CU_TRY(lz_scale_by_norm(qp, w, dim, scr, st));
+    CU_TRY(cudaMemcpyAsync(res, scr + kResZ, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CU_TRY(cudaStreamSynchronize(st));
+    const double a_k = res[0];
+    const double nw2 = res[2];
+    alpha->push_back(a_k);
+    if (nw2 < 1e-24) break;
+    const double b_k = std::sqrt(nw2);
+    beta->push_back(b_k);
+    std::swap(q, qp);  // q_prev <- q ; q <- w / b_k (already written)
+    bprev = b_k;
+  }
+  return FTLM_OK;
+}
+
+}  // namespace
+
+struct ftlm_sector {
+  SectorPlan plan;
+  bool on_device = false;
+  int device = -1;
+  DevSector dev{};
+  std::vector<void*> owned;
+  int apply_path = 0;  // 0 auto, 1 generic, 2 rows+cols
+  LanczosWs ws;
+  DevBuf hx, hy;  // staging for the host-buffer apply
+  cudaStream_t stream = nullptr;
+  ~ftlm_sector() {
+    for (void* p : owned) cudaFree(p);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  int effective_path() const {
+    if (apply_path == 1 || apply_path == 2) return apply_path;
+    return hv_fast_path_ok(dev, plan.max_up_deg) ? 2 : 1;
+  }
+  int apply(const double2* x, double2* y, cudaStream_t st) {
+    const int path = effective_path();
+    if (path == 2 && !hv_fast_path_ok(dev, plan.max_up_deg) && hv_rows_smem_bytes(dev) > 220 * 1024)
+      return fail(FTLM_ERR_UNSUPPORTED, "row pass does not fit in shared memory for this sector");
+    CU_TRY(hv_launch(dev, x, y, path, st));
+    return FTLM_OK;
+  }
+};
+
+namespace {
+
+int upload_plan(ftlm_sector* s) {
+  const SectorPlan& P = s->plan;
+  DevSector& D = s->dev;
+  CU_TRY(cudaGetDevice(&s->device));
+  D.n = P.n;
+  D.Du = P.up.D;
+  D.Dd = P.dn.D;
+  D.dim = P.dim;
+  D.U = P.U;
+  D.V = P.V;
+  std::vector<uint4> w4(static_cast<size_t>(P.up.D));
+  for (size_t i = 0; i < w4.size(); ++i) w4[i] = make_uint4(P.wpl[4 * i], P.wpl[4 * i + 1], P.wpl[4 * i + 2], P.wpl[4 * i + 3]);
+  std::vector<double2> upc(P.up_src.size()), dnc(P.dn_coef.size() / 2);
+  for (size_t i = 0; i < upc.size(); ++i) upc[i] = make_double2(P.up_coef[2 * i], P.up_coef[2 * i + 1]);
+  for (size_t i = 0; i < dnc.size(); ++i) dnc[i] = make_double2(P.dn_coef[2 * i], P.dn_coef[2 * i + 1]);
+  uint32_t *um, *dm, *ulh, *dent, *dnm;
+  int32_t *cuu, *cdd, *uptr, *usrc;
+  uint4* wp;
+  double2 *ucf, *dcf;
+  int64_t* gptr;
+  CU_TRY(upload(P.up.masks, &um, &s->owned));
+  CU_TRY(upload(P.dn.masks, &dm, &s->owned));
+  CU_TRY(upload(P.cnt_uu, &cuu, &s->owned));
+  CU_TRY(upload(P.cnt_dd, &cdd, &s->owned));
+  CU_TRY(upload(w4, &wp, &s->owned));
+  CU_TRY(upload(P.up_ptr, &uptr, &s->owned));
+  CU_TRY(upload(P.up_src, &usrc, &s->owned));
+  CU_TRY(upload(upc, &ucf, &s->owned));
+  CU_TRY(upload(P.up_lohi, &ulh, &s->owned));
+  CU_TRY(upload(P.dn_gptr, &gptr, &s->owned));
+  CU_TRY(upload(P.dn_ent, &dent, &s->owned));
+  CU_TRY(upload(dnc, &dcf, &s->owned));
+  CU_TRY(upload(P.dn_nmask, &dnm, &s->owned));
+  std::vector<int> flags(4, 0);
+  int* fl;
+  CU_TRY(upload(flags, &fl, &s->owned));
+  D.umask = um;
+  D.dmask = dm;
+  D.cnt_uu = cuu;
+  D.cnt_dd = cdd;
+  D.wpl = wp;
+  D.up_ptr = uptr;
+  D.up_src = usrc;
+  D.up_coef = ucf;
+  D.up_lohi = ulh;
+  D.dn_gptr = gptr;
+  D.dn_ent = dent;
+  D.dn_coef = dcf;
+  D.dn_nmask = dnm;
+  D.n_dn_hops = P.dn_pad_hop;
+  D.flags = fl;
+  CU_TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  s->on_device = true;
+  return FTLM_OK;
+}
+
+int create_common(int n_sites, int n_up, int n_dn, double U, double V, const ftlm_hop* hops, int n_hops,
+                  const ftlm_pair* pairs, int n_pairs, bool device, ftlm_sector** out) {
+  if (!out) return fail(FTLM_ERR_INVALID, "null output handle");
+  *out = nullptr;
+  if (n_hops < 0 || n_pairs < 0 || (n_hops > 0 && !hops) || (n_pairs > 0 && !pairs))
+    return fail(FTLM_ERR_INVALID, "bad hopping/pair arrays");
+  std::vector<HopIn> hv(static_cast<size_t>(n_hops));
+  for (int i = 0; i < n_hops; ++i) hv[i] = HopIn{hops[i].from, hops[i].to, hops[i].spin, hops[i].coeff_re, hops[i].coeff_im};
+  std::vector<PairIn> pv(static_cast<size_t>(n_pairs));
+  for (int i = 0; i < n_pairs; ++i) pv[i] = PairIn{pairs[i].i, pairs[i].j};
+  auto* s = new (std::nothrow) ftlm_sector();
+  if (!s) return fail(FTLM_ERR_NOMEM, "host allocation failed");
+  std::string err;
+  try {
+    err = build_plan(n_sites, n_up, n_dn, U, V, hv, pv, &s->plan);
+  } catch (const std::bad_alloc&) {
+    delete s;
+    return fail(FTLM_ERR_NOMEM, "host allocation failed while building the sector plan");
+  }
+  if (!err.empty()) {
+    delete s;
+    const bool unsup = err.find("not supported") != std::string::npos || err.find("2^31") != std::string::npos;
+    return fail(unsup ? FTLM_ERR_UNSUPPORTED : FTLM_ERR_INVALID, err);
+  }
+  if (device) {
+    const int rc = upload_plan(s);
+    if (rc != FTLM_OK) {
+      delete s;
+      return rc;
+    }
+  }
+  *out = s;
+  return FTLM_OK;
+}
+
+int need_device(const ftlm_sector* s) {
+  if (!s) return fail(FTLM_ERR_INVALID, "null sector");
+  if (!s->on_device) return fail(FTLM_ERR_INVALID, "sector was created host-only");
+  return FTLM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ftlm_gpu_last_error(void) { return g_err.c_str(); }
+
+const char* ftlm_gpu_version_string(void) { return "ftlm_extended_hubbard_b200 0.1.0 (sm_100a)"; }
+
+int ftlm_gpu_device_count(int* n) {
+  if (!n) return fail(FTLM_ERR_INVALID, "null");
+  *n = 0;
+  const cudaError_t e = cudaGetDeviceCount(n);
+  if (e != cudaSuccess) {
+    *n = 0;
+    return fail(FTLM_ERR_CUDA, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+  }
+  return FTLM_OK;
+}
+
+int ftlm_gpu_build_geometry(const ftlm_params* p, ftlm_hop* hops, int max_hops, int* n_hops, ftlm_pair* pairs,
+                            int max_pairs, int* n_pairs) {
+  if (!p || !n_hops || !n_pairs) return fail(FTLM_ERR_INVALID, "null argument");
+  if (p->Lx <= 0 || p->Ly <= 0) return fail(FTLM_ERR_INVALID, "Lx, Ly must be positive");
+  std::vector<HopIn> hv;
+  std::vector<PairIn> pv;
+  build_geometry(p->Lx, p->Ly, p->t, p->tp, p->phi_x, p->phi_y, &hv, &pv);
+  *n_hops = static_cast<int>(hv.size());
+  *n_pairs = static_cast<int>(pv.size());
+  for (int i = 0; i < *n_hops && i < max_hops && hops; ++i)
+    hops[i] = ftlm_hop{hv[i].from, hv[i].to, hv[i].spin, hv[i].cre, hv[i].cim};
+  for (int i = 0; i < *n_pairs && i < max_pairs && pairs; ++i) pairs[i] = ftlm_pair{pv[i].i, pv[i].j};
+  return FTLM_OK;
+}
+
+int ftlm_gpu_sector_create_hops(int n_sites, int n_up, int n_dn, double U, double V, const ftlm_hop* hops, int n_hops,
+                                const ftlm_pair* pairs, int n_pairs, ftlm_sector** out) {
+  return create_common(n_sites, n_up, n_dn, U, V, hops, n_hops, pairs, n_pairs, true, out);
+}
+
+int ftlm_gpu_sector_create_host(int n_sites, int n_up, int n_dn, double U, double V, const ftlm_hop* hops, int n_hops,
+                                const ftlm_pair* pairs, int n_pairs, ftlm_sector** out) {
+  return create_common(n_sites, n_up, n_dn, U, V, hops, n_hops, pairs, n_pairs, false, out);
+}
+
+int ftlm_gpu_sector_create(const ftlm_params* p, int n_up, int n_dn, ftlm_sector** out) {
+  if (!p) return fail(FTLM_ERR_INVALID, "null params");
+  if (p->Lx <= 0 || p->Ly <= 0) return fail(FTLM_ERR_INVALID, "Lx, Ly must be positive");
+  std::vector<HopIn> hv;
+  std::vector<PairIn> pv;
+  build_geometry(p->Lx, p->Ly, p->t, p->tp, p->phi_x, p->phi_y, &hv, &pv);
+  std::vector<ftlm_hop> h(hv.size());
+  for (size_t i = 0; i < hv.size(); ++i) h[i] = ftlm_hop{hv[i].from, hv[i].to, hv[i].spin, hv[i].cre, hv[i].cim};
+  std::vector<ftlm_pair> q(pv.size());
+  for (size_t i = 0; i < pv.size(); ++i) q[i] = ftlm_pair{pv[i].i, pv[i].j};
+  return create_common(p->Lx * p->Ly, n_up, n_dn, p->U, p->V, h.data(), static_cast<int>(h.size()), q.data(),
+                       static_cast<int>(q.size()), true, out);
+}
+
+int ftlm_gpu_sector_destroy(ftlm_sector* s) {
+  delete s;
+  return FTLM_OK;
+}
+
+int ftlm_gpu_sector_dim(const ftlm_sector* s, long long* dim) {
+  if (!s || !dim) return fail(FTLM_ERR_INVALID, "null argument");
+  *dim = s->plan.dim;
+  return FTLM_OK;
+}
+
+int ftlm_gpu_sector_masks(const ftlm_sector* s, uint64_t* up, uint64_t* dn) {
+  if (!s || !up || !dn) return fail(FTLM_ERR_INVALID, "null argument");
+  const auto& P = s->plan;
+  for (int64_t r = 0; r < P.up.D; ++r)
+    for (int64_t c = 0; c < P.dn.D; ++c) {
+      up[r * P.dn.D + c] = P.up.masks[static_cast<size_t>(r)];
+      dn[r * P.dn.D + c] = P.dn.masks[static_cast<size_t>(c)];
+    }
+  return FTLM_OK;
+}
+
+int ftlm_gpu_sector_index_of(const ftlm_sector* s, uint64_t up, uint64_t dn, long long* index) {
+  if (!s || !index) return fail(FTLM_ERR_INVALID, "null argument");
+  *index = -1;
+  if ((up >> 32) != 0 || (dn >> 32) != 0) return FTLM_OK;
+  const int64_t ru = s->plan.up.rank(static_cast<uint32_t>(up));
+  const int64_t rd = s->plan.dn.rank(static_cast<uint32_t>(dn));
+  if (ru >= 0 && rd >= 0) *index = ru * s->plan.dn.D + rd;
+  return FTLM_OK;
+}
+
+int ftlm_gpu_sector_stats(const ftlm_sector* s, double* mean_up, double* mean_dn, long long* du, long long* dd) {
+  if (!s) return fail(FTLM_ERR_INVALID, "null sector");
+  if (mean_up) *mean_up = s->plan.mean_up_sources;
+  if (mean_dn) *mean_dn = s->plan.mean_dn_sources;
+  if (du) *du = s->plan.up.D;
+  if (dd) *dd = s->plan.dn.D;
+  return FTLM_OK;
+}
+
+int ftlm_gpu_sector_diag(const ftlm_sector* s, long long index, double* value) {
+  if (!s || !value) return fail(FTLM_ERR_INVALID, "null argument");
+  if (index < 0 || index >= s->plan.dim) return fail(FTLM_ERR_INVALID, "index out of range");
+  *value = plan_diag(s->plan, index / s->plan.dn.D, index % s->plan.dn.D);
+  return FTLM_OK;
+}
+
+int ftlm_gpu_set_apply_path(ftlm_sector* s, int path) {
+  if (!s || path < 0 || path > 2) return fail(FTLM_ERR_INVALID, "bad path");
+  s->apply_path = path;
+  return FTLM_OK;
+}
+
+int ftlm_gpu_apply(ftlm_sector* s, const double* x, double* y, void* stream) {
+  int rc = need_device(s);
+  if (rc) return rc;
+  if (!x || !y) return fail(FTLM_ERR_INVALID, "null vector");
+  if (x == y) return fail(FTLM_ERR_INVALID, "x and y must not alias");
+  return s->apply(reinterpret_cast<const double2*>(x), reinterpret_cast<double2*>(y), static_cast<cudaStream_t>(stream));
+}
+
+int ftlm_gpu_apply_host(ftlm_sector* s, const double* x, double* y) {
+  int rc = need_device(s);
+  if (rc) return rc;
+  if (!x || !y) return fail(FTLM_ERR_INVALID, "null vector");
+  const size_t bytes = static_cast<size_t>(s->plan.dim) * sizeof(double2);
+  if (!s->hx.p) {
+    CU_TRY(s->hx.alloc(bytes));
+    CU_TRY(s->hy.alloc(bytes));
+  }
+  CU_TRY(cudaMemcpyAsync(s->hx.p, x, bytes, cudaMemcpyHostToDevice, s->stream));
+  rc = s->apply(s->hx.as<double2>(), s->hy.as<double2>(), s->stream);
+  if (rc) return rc;
+  CU_TRY(cudaMemcpyAsync(y, s->hy.p, bytes, cudaMemcpyDeviceToHost, s->stream));
+  CU_TRY(cudaStreamSynchronize(s->stream));
+  return FTLM_OK;
+}
+
+int ftlm_gpu_lanczos(ftlm_sector* s, int max_steps, unsigned seed, int start_mode, double* alpha, double* beta,
+                     int* n_beta, int* used) {
+  int rc = need_device(s);
+  if (rc) return rc;
+  std::vector<double> a, b;
+  rc = run_lanczos(
+      s->plan.dim, [s](const double2* x, double2* y, cudaStream_t st) { return s->apply(x, y, st); }, s->ws,
+      max_steps, seed, start_mode, s->stream, &a, &b);
+  if (rc) return rc;
+  if (alpha) std::copy(a.begin(), a.end(), alpha);
+  if (beta) std::copy(b.begin(), b.end(), beta);
+  if (n_beta) *n_beta = static_cast<int>(b.size());
+  if (used) *used = static_cast<int>(a.size());
+  return FTLM_OK;
+}
+
+int ftlm_gpu_lanczos_op(long long dim, ftlm_apply_fn fn, void* ctx, int max_steps, unsigned seed, int start_mode,
+                        double* alpha, double* beta, int* n_beta, int* used) {
+  if (!fn) return fail(FTLM_ERR_INVALID, "null operator");
+  LanczosWs ws;
+  std::vector<double> a, b;
+  const int rc = run_lanczos(
+      dim,
+      [fn, ctx](const double2* x, double2* y, cudaStream_t st) {
+        if (cudaStreamSynchronize(st) != cudaSuccess) return fail(FTLM_ERR_CUDA, "stream sync before operator");
+        fn(reinterpret_cast<const double*>(x), reinterpret_cast<double*>(y), ctx);
+        if (cudaDeviceSynchronize() != cudaSuccess) return fail(FTLM_ERR_CUDA, "operator callback failed");
+        return FTLM_OK;
+      },
+      ws, max_steps, seed, start_mode, nullptr, &a, &b);
+  if (rc) return rc;
+  if (alpha) std::copy(a.begin(), a.end(), alpha);
+  if (beta) std::copy(b.begin(), b.end(), beta);
+  if (n_beta) *n_beta = static_cast<int>(b.size());
+  if (used) *used = static_cast<int>(a.size());
+  return FTLM_OK;
+}
+
+int ftlm_gpu_tridiag_eig(const double* alpha, const double* beta, const int* n, int nc, int ld, int max_rot, double tol,
+                         double* lam, double* w0) {
+  if (nc < 0 || ld <= 0 || !alpha || !beta || !n || !lam || !w0) return fail(FTLM_ERR_INVALID, "bad arguments");
+  if (ld > 160) return fail(FTLM_ERR_UNSUPPORTED, "tridiagonal size > 160 is not supported by the on-chip Jacobi");
+  for (int c = 0; c < nc; ++c)
+    if (n[c] > ld) return fail(FTLM_ERR_INVALID, "chain length exceeds ld");
+  if (nc == 0) return FTLM_OK;
+  const size_t mat = static_cast<size_t>(nc) * ld * sizeof(double);
+  DevBuf da, db, dn, dl, dw;
+  CU_TRY(da.alloc(mat));
+  CU_TRY(db.alloc(mat));
+  CU_TRY(dn.alloc(nc * sizeof(int)));
+  CU_TRY(dl.alloc(mat));
+  CU_TRY(dw.alloc(mat));
+  CU_TRY(cudaMemcpy(da.p, alpha, mat, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(db.p, beta, mat, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(dn.p, n, nc * sizeof(int), cudaMemcpyHostToDevice));
+  CU_TRY(quad_jacobi(da.as<double>(), db.as<double>(), dn.as<int>(), nc, ld, max_rot, tol, dl.as<double>(),
+                     dw.as<double>(), nullptr));
+  CU_TRY(cudaMemcpy(lam, dl.p, mat, cudaMemcpyDeviceToHost));
+  CU_TRY(cudaMemcpy(w0, dw.p, mat, cudaMemcpyDeviceToHost));
+  return FTLM_OK;
+}
+
+int ftlm_gpu_tridiag_quadrature(const double* alpha, const double* beta, const int* n, int nc, int ld,
+                                const double* bts, int n_bt, double* logq, double* energy) {
+  if (nc < 0 || ld <= 0 || n_bt < 0 || !alpha || !beta || !n || !bts || !logq || !energy)
+    return fail(FTLM_ERR_INVALID, "bad arguments");
+  if (ld > 160) return fail(FTLM_ERR_UNSUPPORTED, "tridiagonal size > 160 is not supported by the on-chip Jacobi");
+  if (nc == 0 || n_bt == 0) return FTLM_OK;
+  const size_t mat = static_cast<size_t>(nc) * ld * sizeof(double);
+  const size_t outb = static_cast<size_t>(nc) * n_bt * sizeof(double);
+  DevBuf da, db, dn, dl, dw, dbt, dq, de;
+  CU_TRY(da.alloc(mat));
+  CU_TRY(db.alloc(mat));
+  CU_TRY(dn.alloc(nc * sizeof(int)));
+  CU_TRY(dl.alloc(mat));
+  CU_TRY(dw.alloc(mat));
+  CU_TRY(dbt.alloc(n_bt * sizeof(double)));
+  CU_TRY(dq.alloc(outb));
+  CU_TRY(de.alloc(outb));
+  CU_TRY(cudaMemcpy(da.p, alpha, mat, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(db.p, beta, mat, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(dn.p, n, nc * sizeof(int), cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(dbt.p, bts, n_bt * sizeof(double), cudaMemcpyHostToDevice));
+  CU_TRY(quad_jacobi(da.as<double>(), db.as<double>(), dn.as<int>(), nc, ld, 0, 1e-14, dl.as<double>(), dw.as<double>(),
+                     nullptr));
+  CU_TRY(quad_eval(dl.as<double>(), dw.as<double>(), dn.as<int>(), nc, ld, dbt.as<double>(), n_bt, dq.as<double>(),
+                   de.as<double>(), nullptr));
+  CU_TRY(cudaMemcpy(logq, dq.p, outb, cudaMemcpyDeviceToHost));
+  CU_TRY(cudaMemcpy(energy, de.p, outb, cudaMemcpyDeviceToHost));
+  return FTLM_OK;
+}
+
+int ftlm_gpu_ritz_values(const double* alpha, const double* beta, int n, int k, double* ritz) {
+  if (n <= 0 || k <= 0 || !alpha || !ritz || (n > 1 && !beta)) return fail(FTLM_ERR_INVALID, "bad arguments");
+  k = std::min(k, n);
+  DevBuf da, db, dr;
+  CU_TRY(da.alloc(n * sizeof(double)));
+  CU_TRY(db.alloc(n * sizeof(double)));
+  CU_TRY(dr.alloc(k * sizeof(double)));
+  CU_TRY(cudaMemcpy(da.p, alpha, n * sizeof(double), cudaMemcpyHostToDevice));
+  if (n > 1) CU_TRY(cudaMemcpy(db.p, beta, (n - 1) * sizeof(double), cudaMemcpyHostToDevice));
+  CU_TRY(ritz_bisect(da.as<double>(), db.as<double>(), n, k, dr.as<double>(), nullptr));
+  CU_TRY(cudaMemcpy(ritz, dr.p, k * sizeof(double), cudaMemcpyDeviceToHost));
+  return FTLM_OK;
+}
+
+int ftlm_gpu_lanczos_extrema(ftlm_sector* s, int max_steps, unsigned seed, int start_mode, double* mn, double* mx,
+                             int* steps_used) {
+  if (!mn || !mx) return fail(FTLM_ERR_INVALID, "null output");
+  *mn = 0.0;
+  *mx = 0.0;
+  if (steps_used) *steps_used = 0;
+  std::vector<double> a(std::max(1, max_steps)), b(std::max(1, max_steps));
+  int nb = 0, used = 0;
+  int rc = ftlm_gpu_lanczos(s, max_steps, seed, start_mode, a.data(), b.data(), &nb, &used);
+  if (rc) return rc;
+  if (steps_used) *steps_used = used;
+  if (used == 0) return FTLM_OK;
+  // src/lanczos.cpp:106-123, 211-231: 120 Jacobi rotations, tol 1e-15, on beta[0..used-2].
+  if (used > 160) return fail(FTLM_ERR_UNSUPPORTED, "more than 160 Lanczos steps for the on-chip Jacobi");
+  std::vector<double> lam(static_cast<size_t>(used)), w(static_cast<size_t>(used));
+  std::vector<double> bt(static_cast<size_t>(used), 0.0);
+  for (int i = 0; i + 1 < used && i < nb; ++i) bt[static_cast<size_t>(i)] = b[static_cast<size_t>(i)];
+  int n1 = used;
+  if (used == 1) {
+    *mn = a[0];
+    *mx = a[0];
+    return FTLM_OK;
+  }
+  rc = ftlm_gpu_tridiag_eig(a.data(), bt.data(), &n1, 1, used, 120, 1e-15, lam.data(), w.data());
+  if (rc) return rc;
+  *mn = *std::min_element(lam.begin(), lam.end());
+  *mx = *std::max_element(lam.begin(), lam.end());
+  return FTLM_OK;
+}
+
+int ftlm_gpu_ftlm_sector(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed, int start_mode,
+                         double* lnz, double* energy) {
+  int rc = need_device(s);
+  if (rc) return rc;
+  if (n_bt < 0 || (n_bt > 0 && (!bts || !lnz || !energy))) return fail(FTLM_ERR_INVALID, "bad arguments");
+  const int64_t dim = s->plan.dim;
+  R = std::max(1, R);
+  M = std::max(1, M);
+  if (M > 160) return fail(FTLM_ERR_UNSUPPORTED, "more than 160 Lanczos steps for the on-chip Jacobi");
+  if (dim == 1) {  // src/ftlm_thermo.cpp:219-223: apply H to e_0.
+    const double one[2] = {1.0, 0.0};
+    double h00[2] = {0.0, 0.0};
+    rc = ftlm_gpu_apply_host(s, one, h00);
+    if (rc) return rc;
+    for (int b = 0; b < n_bt; ++b) {
+      lnz[b] = -bts[b] * h00[0];
+      energy[b] = h00[0];
+    }
+    return FTLM_OK;
+  }
+  std::vector<double> A(static_cast<size_t>(R) * M, 0.0), B(static_cast<size_t>(R) * M, 0.0);
+  std::vector<int> nv(static_cast<size_t>(R), 0);
+  for (int r = 0; r < R; ++r) {
+    const unsigned seed_r = seed + static_cast<unsigned>(r) * 100003u;
+    int nb = 0, used = 0;
+    rc = ftlm_gpu_lanczos(s, M, seed_r, start_mode, &A[static_cast<size_t>(r) * M], &B[static_cast<size_t>(r) * M], &nb,
+                          &used);
+    if (rc) return rc;
+    nv[static_cast<size_t>(r)] = used;
+  }
+  std::vector<double> lq(static_cast<size_t>(R) * n_bt), eq(static_cast<size_t>(R) * n_bt);
+  rc = ftlm_gpu_tridiag_quadrature(A.data(), B.data(), nv.data(), R, M, bts, n_bt, lq.data(), eq.data());
+  if (rc) return rc;
+  DevBuf dq, de, dn, dz, den;
+  CU_TRY(dq.alloc(lq.size() * sizeof(double)));
+  CU_TRY(de.alloc(eq.size() * sizeof(double)));
+  CU_TRY(dn.alloc(nv.size() * sizeof(int)));
+  CU_TRY(dz.alloc(n_bt * sizeof(double)));
+  CU_TRY(den.alloc(n_bt * sizeof(double)));
+  CU_TRY(cudaMemcpy(dq.p, lq.data(), lq.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(de.p, eq.data(), eq.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(dn.p, nv.data(), nv.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CU_TRY(quad_sector(dq.as<double>(), de.as<double>(), dn.as<int>(), R, n_bt, std::log(static_cast<double>(dim)),
+                     dz.as<double>(), den.as<double>(), nullptr));
+  CU_TRY(cudaMemcpy(lnz, dz.p, n_bt * sizeof(double), cudaMemcpyDeviceToHost));
+  CU_TRY(cudaMemcpy(energy, den.p, n_bt * sizeof(double), cudaMemcpyDeviceToHost));
+  return FTLM_OK;
+}
+
+int ftlm_gpu_gc_reduce(const double* lnz_s, const double* e_s, const int* N_s, int n_sec, const double* bts, int n_bt,
+                       const double* mus, int n_mu, int n_sites, double* lnz_gc, double* n_avg, double* e_avg) {
+  if (n_sec < 0 || n_bt < 0 || n_mu < 0 || !lnz_s || !e_s || !N_s || !bts || !mus || !lnz_gc || !n_avg || !e_avg)
+    return fail(FTLM_ERR_INVALID, "bad arguments");
+  if (n_bt == 0 || n_mu == 0) return FTLM_OK;
+  const size_t sb = static_cast<size_t>(std::max(n_sec, 1)) * n_bt * sizeof(double);
+  const size_t gb = static_cast<size_t>(n_bt) * n_mu * sizeof(double);
+  DevBuf dl, de, dN, db, dm, o1, o2, o3;
+  CU_TRY(dl.alloc(sb));
+  CU_TRY(de.alloc(sb));
+  CU_TRY(dN.alloc(std::max(n_sec, 1) * sizeof(int)));
+  CU_TRY(db.alloc(n_bt * sizeof(double)));
+  CU_TRY(dm.alloc(n_mu * sizeof(double)));
+  CU_TRY(o1.alloc(gb));
+  CU_TRY(o2.alloc(gb));
+  CU_TRY(o3.alloc(gb));
+  if (n_sec > 0) {
+    CU_TRY(cudaMemcpy(dl.p, lnz_s, static_cast<size_t>(n_sec) * n_bt * sizeof(double), cudaMemcpyHostToDevice));
+    CU_TRY(cudaMemcpy(de.p, e_s, static_cast<size_t>(n_sec) * n_bt * sizeof(double), cudaMemcpyHostToDevice));
+    CU_TRY(cudaMemcpy(dN.p, N_s, n_sec * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  CU_TRY(cudaMemcpy(db.p, bts, n_bt * sizeof(double), cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(dm.p, mus, n_mu * sizeof(double), cudaMemcpyHostToDevice));
+  CU_TRY(gc_reduce_dev(dl.as<double>(), de.as<double>(), dN.as<int>(), n_sec, db.as<double>(), n_bt, dm.as<double>(),
+                       n_mu, n_sites, o1.as<double>(), o2.as<double>(), o3.as<double>(), nullptr));
+  CU_TRY(cudaMemcpy(lnz_gc, o1.p, gb, cudaMemcpyDeviceToHost));
+  CU_TRY(cudaMemcpy(n_avg, o2.p, gb, cudaMemcpyDeviceToHost));
+  CU_TRY(cudaMemcpy(e_avg, o3.p, gb, cudaMemcpyDeviceToHost));
+  return FTLM_OK;
+}
+
+int ftlm_gpu_gc_sweep(const ftlm_params* p, int R, int M, unsigned seed, int start_mode, const double* bts, int n_bt,
+                      const double* mus, int n_mu, double* lnz_s, double* e_s, double* lnz_gc, double* n_avg,
+                      double* e_avg) {
+  if (!p || !lnz_s || !e_s) return fail(FTLM_ERR_INVALID, "null argument");
+  const int n = p->Lx * p->Ly;
+  if (n <= 0 || n > 32) return fail(FTLM_ERR_INVALID, "FockBasis: require 1 <= n_sites <= 32 (bit packing)");
+  const int nsec = (n + 1) * (n + 1);
+  std::vector<int> N(static_cast<size_t>(nsec));
+  for (int nu = 0; nu <= n; ++nu)
+    for (int nd = 0; nd <= n; ++nd) {
+      const int idx = nu * (n + 1) + nd;  // benchmarks/bench_ftlm_nmu_rect.cpp:62
+      N[static_cast<size_t>(idx)] = nu + nd;
+      ftlm_sector* s = nullptr;
+      int rc = ftlm_gpu_sector_create(p, nu, nd, &s);
+      if (rc) return rc;
+      rc = ftlm_gpu_ftlm_sector(s, bts, n_bt, R, M, seed, start_mode, lnz_s + static_cast<size_t>(idx) * n_bt,
+                                e_s + static_cast<size_t>(idx) * n_bt);
+      ftlm_gpu_sector_destroy(s);
+      if (rc) return rc;
+    }
+  if (lnz_gc && n_avg && e_avg)
+    return ftlm_gpu_gc_reduce(lnz_s, e_s, N.data(), nsec, bts, n_bt, mus, n_mu, n, lnz_gc, n_avg, e_avg);
+  return FTLM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,62 @@
+// Device-side view of a sector plan (see plan.hpp) and small helpers shared by the kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ftlm_b200 {
+
+struct DevSector {
+  int n;
+  int64_t Du, Dd, dim;
+  double U, V;
+  const uint32_t* umask;   // [Du]
+  const uint32_t* dmask;   // [Dd]
+  const int32_t* cnt_uu;   // [Du]
+  const int32_t* cnt_dd;   // [Dd]
+  const uint4* wpl;        // [Du]
+  const int32_t* up_ptr;   // [Du+1]
+  const int32_t* up_src;   // [nnz_up]
+  const double2* up_coef;  // [nnz_up]
+  const uint32_t* up_lohi; // [nnz_up]
+  const int64_t* dn_gptr;  // [ngroups+1]
+  const uint32_t* dn_ent;  // ELL entries
+  const double2* dn_coef;  // [n_dn_hops+1]
+  const uint32_t* dn_nmask;// [n_dn_hops+1]
+  int n_dn_hops;           // == pad hop id
+  int* flags;              // [0]: input has a non-zero entry with |x|^2 < 1e-28
+};
+
+// The reference skips source columns with std::norm(x) < 1e-28
+// (src/hubbard_hamiltonian.cpp:62); a skipped source contributes exactly nothing.
+__device__ __forceinline__ bool tiny(double2 v) { return v.x * v.x + v.y * v.y < 1e-28; }
+
+// Inclusive prefix XOR of the down string, shifted left by one: bit k = parity(#dn in [0,k)).
+__device__ __forceinline__ uint32_t prefix_parity_shifted(uint32_t d) {
+  uint32_t p = d;
+  p ^= p << 1;
+  p ^= p << 2;
+  p ^= p << 4;
+  p ^= p << 8;
+  p ^= p << 16;
+  return p << 1;
+}
+
+__device__ __forceinline__ double diag_value(const DevSector& S, uint32_t u, uint32_t d, int cuu, int cdd, uint4 w) {
+  const int cross = __popc(d & w.x) + 2 * __popc(d & w.y) + 4 * __popc(d & w.z) + 8 * __popc(d & w.w);
+  return S.U * static_cast<double>(__popc(u & d)) + S.V * static_cast<double>(cuu + cdd + cross);
+}
+
+// acc += (neg ? -c : c) * v   (complex)
+__device__ __forceinline__ void cmac(double2& acc, double2 c, double2 v, uint32_t neg) {
+  if (neg) {
+    c.x = -c.x;
+    c.y = -c.y;
+  }
+  acc.x = fma(c.x, v.x, acc.x);
+  acc.x = fma(-c.y, v.y, acc.x);
+  acc.y = fma(c.x, v.y, acc.y);
+  acc.y = fma(c.y, v.x, acc.y);
+}
+
+}  // namespace ftlm_b200

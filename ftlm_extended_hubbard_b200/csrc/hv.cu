@@ -1,0 +1,221 @@
+// H·v kernels for one (N_up, N_dn) sector, complex128.  State (ru, rd) lives at ru*Dd + rd,
+// so the vector is a Du x Dd row-major matrix X[up string][down string].
+//
+//   H X = diag o X  +  (down hops: mix columns inside a row)  +  (up hops: mix rows, column-wise)
+//
+// Paths:
+//   hv_generic  one thread per output element, everything gathered from global memory.  Any size.
+//   hv_rows     pass 1 of the fast path: persistent CTAs, one output row at a time; the input
+//               row is staged in shared memory (down hops gather inside it); writes
+//               y = diag o x + down part.  Requires a down row (+ coefficient table) to fit in SMEM.
+//   hv_cols     pass 2: CTA = (output row, 256-column chunk), chunk-major launch order so that
+//               the 256-column slab of x stays resident in L2 while all rows read it; adds the
+//               up part: y[r, c] += sum_j coef_j * s_j(c) * x[src_j, c].
+// Reference: src/hubbard_hamiltonian.cpp:51-108 (apply_extended_hubbard).
+#include <algorithm>
+
+#include "device.cuh"
+#include "hv.cuh"
+
+namespace ftlm_b200 {
+
+namespace {
+
+__global__ void __launch_bounds__(256) hv_generic_kernel(DevSector S, const double2* __restrict__ x,
+                                                         double2* __restrict__ y) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; idx < S.dim; idx += stride) {
+    const int64_t r = idx / S.Dd;
+    const int64_t c = idx - r * S.Dd;
+    const uint32_t u = S.umask[r];
+    const uint32_t d = S.dmask[c];
+    double2 acc = make_double2(0.0, 0.0);
+    const double2 xv = x[idx];
+    if (!tiny(xv)) {
+      const double dg = diag_value(S, u, d, S.cnt_uu[r], S.cnt_dd[c], S.wpl[r]);
+      acc.x = dg * xv.x;
+      acc.y = dg * xv.y;
+    }
+    // down hops: sources inside row r
+    const double2* xrow = x + r * S.Dd;
+    const int64_t g = c >> 5;
+    const int lane = static_cast<int>(c & 31);
+    const int64_t e_end = S.dn_gptr[g + 1];
+    for (int64_t p = S.dn_gptr[g] + lane; p < e_end; p += 32) {
+      const uint32_t ent = S.dn_ent[p];
+      const int h = static_cast<int>((ent >> 1) & 511u);
+      if (h == S.n_dn_hops) continue;
+      const double2 xs = xrow[ent >> 10];
+      if (tiny(xs)) continue;
+      const uint32_t neg = (ent & 1u) ^ (static_cast<uint32_t>(__popc(u & S.dn_nmask[h])) & 1u);
+      cmac(acc, S.dn_coef[h], xs, neg);
+    }
+    // up hops: sources in other rows, same column
+    const uint32_t q = prefix_parity_shifted(d);
+    const int j_end = S.up_ptr[r + 1];
+    for (int j = S.up_ptr[r]; j < j_end; ++j) {
+      const double2 xs = x[static_cast<int64_t>(S.up_src[j]) * S.Dd + c];
+      if (tiny(xs)) continue;
+      const uint32_t lh = S.up_lohi[j];
+      const uint32_t neg = ((q >> (lh & 255u)) ^ (q >> (lh >> 8))) & 1u;
+      cmac(acc, S.up_coef[j], xs, neg);
+    }
+    y[idx] = acc;
+  }
+}
+
+constexpr int kRowThreads = 1024;
+
+__global__ void __launch_bounds__(kRowThreads, 1) hv_rows_kernel(DevSector S, const double2* __restrict__ x,
+                                                                   double2* __restrict__ y) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int Dd = static_cast<int>(S.Dd);
+  double2* xs = reinterpret_cast<double2*>(smem_raw);
+  double2* coef = xs + Dd;
+  const int tid = threadIdx.x;
+  for (int64_t r = blockIdx.x; r < S.Du; r += gridDim.x) {
+    // Warm L2 with the row this CTA handles next (bulk prefetch, no completion to wait on).
+    if (tid == 0 && r + gridDim.x < S.Du) {
+      const char* nxt = reinterpret_cast<const char*>(x + (r + gridDim.x) * S.Dd);
+      const uint32_t bytes = static_cast<uint32_t>(S.Dd * sizeof(double2));
+      for (uint32_t off = 0; off < bytes; off += 32768u) {
+        const uint32_t sz = min(32768u, bytes - off);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(nxt + off), "r"(sz) : "memory");
+      }
+    }
+    const uint32_t u = S.umask[r];
+    const int cuu = S.cnt_uu[r];
+    const uint4 w = S.wpl[r];
+    const double2* xrow = x + r * S.Dd;
+    int saw_tiny = 0;
+    for (int c = tid; c < Dd; c += kRowThreads) {
+      double2 v = xrow[c];
+      if (tiny(v)) {
+        saw_tiny |= (v.x != 0.0 || v.y != 0.0);
+        v = make_double2(0.0, 0.0);
+      }
+      xs[c] = v;
+    }
+    for (int h = tid; h <= S.n_dn_hops; h += kRowThreads) {
+      double2 cf = S.dn_coef[h];
+      if (__popc(u & S.dn_nmask[h]) & 1) {
+        cf.x = -cf.x;
+        cf.y = -cf.y;
+      }
+      coef[h] = cf;
+    }
+    if (saw_tiny) atomicOr(S.flags, 1);
+    __syncthreads();
+    double2* yrow = y + r * S.Dd;
+    for (int c = tid; c < Dd; c += kRowThreads) {
+      const double2 xv = xs[c];
+      const double dg = diag_value(S, u, S.dmask[c], cuu, S.cnt_dd[c], w);
+      double2 acc = make_double2(dg * xv.x, dg * xv.y);
+      const int g = c >> 5;
+      const int64_t e_end = S.dn_gptr[g + 1];
+#pragma unroll 4
+      for (int64_t p = S.dn_gptr[g] + (c & 31); p < e_end; p += 32) {
+        const uint32_t ent = __ldg(S.dn_ent + p);
+        cmac(acc, coef[(ent >> 1) & 511u], xs[ent >> 10], ent & 1u);
+      }
+      yrow[c] = acc;
+    }
+    __syncthreads();
+  }
+}
+
+constexpr int kColThreads = 256;
+constexpr int kMaxUpDeg = 128;
+
+template <bool kFilter>
+__device__ __forceinline__ void cols_body(const DevSector& S, const double2* __restrict__ x, double2* __restrict__ y,
+                                          int64_t r, int64_t c, int deg, const int* s_src, const double2* s_coef,
+                                          const uint32_t* s_lh) {
+  const uint32_t q = prefix_parity_shifted(S.dmask[c]);
+  double2 acc = y[r * S.Dd + c];
+  const double2* xc = x + c;
+  int j = 0;
+  for (; j + 8 <= deg; j += 8) {
+    double2 v[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) v[t] = xc[static_cast<int64_t>(s_src[j + t]) * S.Dd];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      if (kFilter && tiny(v[t])) continue;
+      const uint32_t lh = s_lh[j + t];
+      cmac(acc, s_coef[j + t], v[t], ((q >> (lh & 255u)) ^ (q >> (lh >> 8))) & 1u);
+    }
+  }
+  for (; j < deg; ++j) {
+    const double2 v = xc[static_cast<int64_t>(s_src[j]) * S.Dd];
+    if (kFilter && tiny(v)) continue;
+    const uint32_t lh = s_lh[j];
+    cmac(acc, s_coef[j], v, ((q >> (lh & 255u)) ^ (q >> (lh >> 8))) & 1u);
+  }
+  y[r * S.Dd + c] = acc;
+}
+
+__global__ void __launch_bounds__(kColThreads) hv_cols_kernel(DevSector S, const double2* __restrict__ x,
+                                                              double2* __restrict__ y) {
+  __shared__ int s_src[kMaxUpDeg];
+  __shared__ double2 s_coef[kMaxUpDeg];
+  __shared__ uint32_t s_lh[kMaxUpDeg];
+  const int64_t b = blockIdx.x;
+  const int64_t chunk = b / S.Du;
+  const int64_t r = b - chunk * S.Du;
+  const int j0 = S.up_ptr[r];
+  const int deg = S.up_ptr[r + 1] - j0;
+  for (int j = threadIdx.x; j < deg; j += kColThreads) {
+    s_src[j] = S.up_src[j0 + j];
+    s_coef[j] = S.up_coef[j0 + j];
+    s_lh[j] = S.up_lohi[j0 + j];
+  }
+  const bool filt = (*S.flags) != 0;
+  __syncthreads();
+  const int64_t c = chunk * kColThreads + threadIdx.x;
+  if (c >= S.Dd) return;
+  if (filt)
+    cols_body<true>(S, x, y, r, c, deg, s_src, s_coef, s_lh);
+  else
+    cols_body<false>(S, x, y, r, c, deg, s_src, s_coef, s_lh);
+}
+
+int g_num_sms = 0;
+
+}  // namespace
+
+size_t hv_rows_smem_bytes(const DevSector& S) {
+  return static_cast<size_t>(S.Dd) * sizeof(double2) + static_cast<size_t>(S.n_dn_hops + 1) * sizeof(double2);
+}
+
+bool hv_fast_path_ok(const DevSector& S, int max_up_deg) {
+  return hv_rows_smem_bytes(S) <= 220 * 1024 && max_up_deg <= kMaxUpDeg && S.dim >= (1 << 16);
+}
+
+cudaError_t hv_launch(const DevSector& S, const double2* x, double2* y, int path, cudaStream_t st) {
+  if (S.dim <= 0) return cudaSuccess;
+  if (g_num_sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_num_sms <= 0) g_num_sms = 148;
+  }
+  if (path == 2) {
+    cudaError_t e = cudaMemsetAsync(S.flags, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    const size_t sm = hv_rows_smem_bytes(S);
+    e = cudaFuncSetAttribute(hv_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
+    if (e != cudaSuccess) return e;
+    const int grid_r = static_cast<int>(std::min<int64_t>(S.Du, g_num_sms));
+    hv_rows_kernel<<<grid_r, kRowThreads, sm, st>>>(S, x, y);
+    const int64_t nchunks = (S.Dd + kColThreads - 1) / kColThreads;
+    const int64_t grid_c = nchunks * S.Du;
+    hv_cols_kernel<<<static_cast<unsigned>(grid_c), kColThreads, 0, st>>>(S, x, y);
+    return cudaGetLastError();
+  }
+  const int64_t blocks = std::min<int64_t>((S.dim + 255) / 256, static_cast<int64_t>(g_num_sms) * 16);
+  hv_generic_kernel<<<static_cast<unsigned>(blocks), 256, 0, st>>>(S, x, y);
+  return cudaGetLastError();
+}
+
+}  // namespace ftlm_b200

@@ -1,0 +1,311 @@
+// Host-side sector plan; see plan.hpp for the conventions.
+#include "plan.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <map>
+#include <utility>
+
+namespace ftlm_b200 {
+
+namespace {
+
+uint64_t g_binom[65][65];
+bool g_binom_ready = false;
+
+void init_binom() {
+  if (g_binom_ready) return;
+  for (int n = 0; n <= 64; ++n) {
+    for (int k = 0; k <= 64; ++k) g_binom[n][k] = 0;
+    g_binom[n][0] = 1;
+    for (int k = 1; k <= n; ++k) g_binom[n][k] = g_binom[n - 1][k - 1] + (k <= n - 1 ? g_binom[n - 1][k] : 0);
+  }
+  g_binom_ready = true;
+}
+
+// Reference src/fock_basis.cpp:7-15: lexicographic k-subsets (lowest free position first).
+void enumerate(int n, int k, int pos, uint32_t cur, std::vector<uint32_t>* out) {
+  if (k == 0) {
+    out->push_back(cur);
+    return;
+  }
+  for (int i = pos; i <= n - k; ++i) enumerate(n, k - 1, i + 1, cur | (1u << i), out);
+}
+
+inline int popc(uint32_t x) { return __builtin_popcount(x); }
+
+inline uint32_t range_mask(int a, int b) {  // sites a..b-1 (a <= b)
+  const uint64_t hi = (b >= 32) ? 0xFFFFFFFFull : ((1ull << b) - 1);
+  const uint64_t lo = (a >= 32) ? 0xFFFFFFFFull : ((1ull << a) - 1);
+  return static_cast<uint32_t>(hi & ~lo);
+}
+
+// Merge directed hops of one spin by (from, to), summing coefficients in list order.
+std::vector<MergedHop> merge_hops(const std::vector<HopIn>& hops, int spin) {
+  std::vector<MergedHop> out;
+  std::map<std::pair<int, int>, size_t> where;
+  for (const auto& h : hops) {
+    if (h.spin != spin) continue;
+    const auto key = std::make_pair(h.from, h.to);
+    auto it = where.find(key);
+    if (it == where.end()) {
+      where[key] = out.size();
+      MergedHop m{};
+      m.from = h.from;
+      m.to = h.to;
+      m.cre = h.cre;
+      m.cim = h.cim;
+      out.push_back(m);
+    } else {
+      out[it->second].cre += h.cre;
+      out[it->second].cim += h.cim;
+    }
+  }
+  for (auto& m : out) {
+    m.lo = std::min(m.from, m.to);
+    m.hi = std::max(m.from, m.to);
+    m.own_mask = range_mask(m.lo + 1, m.hi);
+    // up hop: other species (down) counted on [lo, hi); down hop: up counted on (lo, hi].
+    m.other_mask = (spin == 0) ? range_mask(m.lo, m.hi) : range_mask(m.lo + 1, m.hi + 1);
+  }
+  return out;
+}
+
+}  // namespace
+
+uint64_t binom(int n, int k) {
+  init_binom();
+  if (n < 0 || k < 0 || k > n || n > 64) return 0;
+  return g_binom[n][k];
+}
+
+void SpinSpace::build(int n_, int k_) {
+  init_binom();
+  n = n_;
+  k = k_;
+  masks.clear();
+  masks.reserve(static_cast<size_t>(binom(n, k)));
+  enumerate(n, k, 0, 0u, &masks);
+  D = static_cast<int64_t>(masks.size());
+}
+
+int64_t SpinSpace::rank(uint32_t m) const {
+  if (n < 32 && (m >> n) != 0) return -1;
+  if (popc(m) != k) return -1;
+  // colex rank of the bit-reversed set: sum_j C(q_j, j), q ascending, j = 1..k.
+  uint64_t colex = 0;
+  int j = 0;
+  for (int q = 0; q < n; ++q) {
+    const int p = n - 1 - q;
+    if ((m >> p) & 1u) {
+      ++j;
+      colex += g_binom[q][j];
+    }
+  }
+  return static_cast<int64_t>(binom(n, k) - 1 - colex);
+}
+
+void build_geometry(int Lx, int Ly, double t, double tp, double phix, double phiy, std::vector<HopIn>* hops,
+                    std::vector<PairIn>* pairs) {
+  hops->clear();
+  pairs->clear();
+  auto site = [Lx](int x, int y) { return y * Lx + x; };
+  auto bond = [hops](int from, int to, std::complex<double> phase, double ts) {
+    if (std::abs(ts) < 1e-15) return;
+    const std::complex<double> cij = -ts * phase, cji = -ts * std::conj(phase);
+    for (int s = 0; s < 2; ++s) {
+      hops->push_back(HopIn{from, to, s, cij.real(), cij.imag()});
+      hops->push_back(HopIn{to, from, s, cji.real(), cji.imag()});
+    }
+  };
+  auto phase = [phix, phiy](int wx, int wy) {
+    return std::polar(1.0, static_cast<double>(wx) * phix + static_cast<double>(wy) * phiy);
+  };
+  auto nn = [pairs](int a, int b) {
+    if (a == b) return;
+    if (a > b) std::swap(a, b);
+    pairs->push_back(PairIn{a, b});
+  };
+  for (int y = 0; y < Ly; ++y) {
+    for (int x = 0; x < Lx; ++x) {
+      const int i = site(x, y);
+      if (Lx > 1) {
+        const bool w = x + 1 >= Lx;
+        const int j = site(w ? 0 : x + 1, y);
+        if (i != j) {
+          nn(i, j);
+          bond(i, j, phase(w ? 1 : 0, 0), t);
+        }
+      }
+      if (Ly > 1) {
+        const bool w = y + 1 >= Ly;
+        const int j = site(x, w ? 0 : y + 1);
+        if (i != j) {
+          nn(i, j);
+          bond(i, j, phase(0, w ? 1 : 0), t);
+        }
+      }
+      static const int dd[4][2] = {{1, 1}, {1, -1}, {-1, 1}, {-1, -1}};
+      for (const auto& d : dd) {
+        int nx = x + d[0], ny = y + d[1], wx = 0, wy = 0;
+        if (nx >= Lx) {
+          nx -= Lx;
+          wx = 1;
+        } else if (nx < 0) {
+          nx += Lx;
+          wx = -1;
+        }
+        if (ny >= Ly) {
+          ny -= Ly;
+          wy = 1;
+        } else if (ny < 0) {
+          ny += Ly;
+          wy = -1;
+        }
+        const int j = site(nx, ny);
+        if (i != j) bond(i, j, phase(wx, wy), tp);
+      }
+    }
+  }
+}
+
+double plan_diag(const SectorPlan& p, int64_t ru, int64_t rd) {
+  const uint32_t u = p.up.masks[static_cast<size_t>(ru)], d = p.dn.masks[static_cast<size_t>(rd)];
+  const uint32_t* w = &p.wpl[static_cast<size_t>(ru) * 4];
+  const int cross = popc(d & w[0]) + 2 * popc(d & w[1]) + 4 * popc(d & w[2]) + 8 * popc(d & w[3]);
+  const int vcount = p.cnt_uu[static_cast<size_t>(ru)] + p.cnt_dd[static_cast<size_t>(rd)] + cross;
+  return p.U * static_cast<double>(popc(u & d)) + p.V * static_cast<double>(vcount);
+}
+
+std::string build_plan(int n_sites, int n_up, int n_dn, double U, double V, const std::vector<HopIn>& hops,
+                       const std::vector<PairIn>& pairs, SectorPlan* out) {
+  init_binom();
+  if (n_sites <= 0 || n_sites > 32) return "FockBasis: require 1 <= n_sites <= 32 (bit packing)";
+  if (n_up < 0 || n_dn < 0 || n_up > n_sites || n_dn > n_sites) return "FockBasis: particle numbers out of range";
+  for (const auto& h : hops) {
+    if (h.from < 0 || h.to < 0 || h.from >= n_sites || h.to >= n_sites || (h.spin != 0 && h.spin != 1))
+      return "hopping out of range";
+    if (h.from == h.to) return "on-site hopping entries are not supported";
+  }
+  for (const auto& pr : pairs)
+    if (pr.i < 0 || pr.j < 0 || pr.i >= n_sites || pr.j >= n_sites) return "nn pair out of range";
+  const uint64_t Du = binom(n_sites, n_up), Dd = binom(n_sites, n_dn);
+  if (Du > (1u << 22) || Dd > (1u << 22)) return "spin space larger than 2^22 strings is not supported";
+  if (Du * Dd >= (1ull << 31)) return "sector dimension must fit the reference's int index (< 2^31)";
+
+  SectorPlan& P = *out;
+  P = SectorPlan{};
+  P.n = n_sites;
+  P.nu = n_up;
+  P.nd = n_dn;
+  P.U = U;
+  P.V = V;
+  P.pairs = pairs;
+  P.up.build(n_sites, n_up);
+  P.dn.build(n_sites, n_dn);
+  P.dim = P.up.D * P.dn.D;
+  P.hu = merge_hops(hops, 0);
+  P.hd = merge_hops(hops, 1);
+  if (P.hd.size() + 1 > 511) return "more than 510 distinct down hoppings are not supported";
+
+  // Diagonal tables.  sum_pairs (u_i+d_i)(u_j+d_j) = uu + dd + sum_s d_s * c_u(s).
+  P.cnt_uu.resize(static_cast<size_t>(P.up.D));
+  P.cnt_dd.resize(static_cast<size_t>(P.dn.D));
+  P.wpl.assign(static_cast<size_t>(P.up.D) * 4, 0u);
+  for (int64_t r = 0; r < P.up.D; ++r) {
+    const uint32_t u = P.up.masks[static_cast<size_t>(r)];
+    int uu = 0;
+    int cu[32] = {0};
+    for (const auto& pr : pairs) {
+      const int ui = (u >> pr.i) & 1u, uj = (u >> pr.j) & 1u;
+      uu += ui * uj;
+      cu[pr.i] += uj;
+      cu[pr.j] += ui;
+    }
+    P.cnt_uu[static_cast<size_t>(r)] = uu;
+    for (int s = 0; s < n_sites; ++s) {
+      if (cu[s] > 15) return "more than 15 nn pairs on one site are not supported";
+      for (int b = 0; b < 4; ++b)
+        if ((cu[s] >> b) & 1) P.wpl[static_cast<size_t>(r) * 4 + b] |= (1u << s);
+    }
+  }
+  for (int64_t r = 0; r < P.dn.D; ++r) {
+    const uint32_t d = P.dn.masks[static_cast<size_t>(r)];
+    int dd = 0;
+    for (const auto& pr : pairs) dd += static_cast<int>(((d >> pr.i) & 1u) * ((d >> pr.j) & 1u));
+    P.cnt_dd[static_cast<size_t>(r)] = dd;
+  }
+
+  // Up part: for output up string u', hop f->t contributes from source u = u' ^ f ^ t when
+  // u' has t and not f; the up-string factor (-1)^#up(lo,hi) is the same on u and u'.
+  P.up_ptr.assign(static_cast<size_t>(P.up.D) + 1, 0);
+  for (int64_t r = 0; r < P.up.D; ++r) {
+    const uint32_t u2 = P.up.masks[static_cast<size_t>(r)];
+    int deg = 0;
+    for (const auto& h : P.hu) {
+      if (!((u2 >> h.to) & 1u) || ((u2 >> h.from) & 1u)) continue;
+      const uint32_t u = u2 ^ (1u << h.from) ^ (1u << h.to);
+      const int64_t src = P.up.rank(u);
+      if (src < 0) return "internal: up source rank";
+      const double sg = (popc(u & h.own_mask) & 1) ? -1.0 : 1.0;
+      P.up_src.push_back(static_cast<int32_t>(src));
+      P.up_coef.push_back(sg * h.cre);
+      P.up_coef.push_back(sg * h.cim);
+      P.up_lohi.push_back(static_cast<uint32_t>(h.lo) | (static_cast<uint32_t>(h.hi) << 8));
+      ++deg;
+    }
+    P.max_up_deg = std::max(P.max_up_deg, deg);
+    P.up_ptr[static_cast<size_t>(r) + 1] = static_cast<int32_t>(P.up_src.size());
+  }
+  P.mean_up_sources = P.up.D ? static_cast<double>(P.up_src.size()) / static_cast<double>(P.up.D) : 0.0;
+
+  // Down part: per output down string d', hop f->t contributes from d = d' ^ f ^ t; the
+  // down-string factor (-1)^#dn(lo,hi) goes into the entry, the up-string factor per row.
+  const int nh = static_cast<int>(P.hd.size());
+  P.dn_pad_hop = nh;
+  P.dn_coef.assign(static_cast<size_t>(nh + 1) * 2, 0.0);
+  P.dn_nmask.assign(static_cast<size_t>(nh + 1), 0u);
+  for (int h = 0; h < nh; ++h) {
+    P.dn_coef[2 * h] = P.hd[h].cre;
+    P.dn_coef[2 * h + 1] = P.hd[h].cim;
+    P.dn_nmask[h] = P.hd[h].other_mask;
+  }
+  const int64_t ngroups = (P.dn.D + 31) / 32;
+  P.dn_gptr.assign(static_cast<size_t>(ngroups) + 1, 0);
+  std::vector<std::vector<uint32_t>> lane(32);
+  int64_t total_src = 0;
+  for (int64_t g = 0; g < ngroups; ++g) {
+    size_t K = 0;
+    for (int l = 0; l < 32; ++l) {
+      lane[l].clear();
+      const int64_t r = g * 32 + l;
+      if (r >= P.dn.D) continue;
+      const uint32_t d2 = P.dn.masks[static_cast<size_t>(r)];
+      for (int h = 0; h < nh; ++h) {
+        const auto& hp = P.hd[h];
+        if (!((d2 >> hp.to) & 1u) || ((d2 >> hp.from) & 1u)) continue;
+        const uint32_t d = d2 ^ (1u << hp.from) ^ (1u << hp.to);
+        const int64_t src = P.dn.rank(d);
+        if (src < 0) return "internal: down source rank";
+        const uint32_t sg = static_cast<uint32_t>(popc(d & hp.own_mask) & 1);
+        lane[l].push_back((static_cast<uint32_t>(src) << 10) | (static_cast<uint32_t>(h) << 1) | sg);
+      }
+      total_src += static_cast<int64_t>(lane[l].size());
+      P.max_dn_deg = std::max(P.max_dn_deg, static_cast<int>(lane[l].size()));
+      K = std::max(K, lane[l].size());
+    }
+    for (size_t k = 0; k < K; ++k)
+      for (int l = 0; l < 32; ++l) {
+        const int64_t r = g * 32 + l;
+        const uint32_t self = static_cast<uint32_t>(r < P.dn.D ? r : 0);
+        P.dn_ent.push_back(k < lane[l].size() ? lane[l][k]
+                                              : ((self << 10) | (static_cast<uint32_t>(P.dn_pad_hop) << 1)));
+      }
+    P.dn_gptr[static_cast<size_t>(g) + 1] = static_cast<int64_t>(P.dn_ent.size());
+  }
+  P.mean_dn_sources = P.dn.D ? static_cast<double>(total_src) / static_cast<double>(P.dn.D) : 0.0;
+  return "";
+}
+
+}  // namespace ftlm_b200

@@ -1,0 +1,97 @@
+// Host-side sector plan: the (N_up, N_dn) Fock basis in factorised form and the gather
+// tables the device kernels read.  Pure C++ (no CUDA), so its integer work is checkable on CPU.
+//
+// Basis (reference src/fock_basis.cpp:17-42): strings of one spin species are the k-subsets
+// of the n sites in lexicographic order of their sorted site lists; state index =
+// rank_up * C(n, n_dn) + rank_dn.  Here the two string lists are kept separately (the state
+// is never materialised as a dim-long mask pair) and ranks come from a closed form instead of
+// a hash map: lex_rank(m) = C(n,k) - 1 - colex_rank(bitreverse_n(m)).
+//
+// Operator (reference src/hubbard_hamiltonian.cpp:51-108), gather form, per spin species:
+//   up hop  f->t (lo<hi the two sites): JW sign = (-1)^(#up in (lo,hi) + #dn in [lo,hi))
+//   dn hop  f->t                      : JW sign = (-1)^(#up in (lo,hi] + #dn in (lo,hi))
+// The factor that depends only on the moving species' string is folded into the table
+// coefficient; the factor that depends on the other species' string is applied per element
+// (up part: from the prefix parity of the down string; down part: per up row, per hop).
+// Duplicate directed hops (same spin, from, to) are merged by summing their coefficients in
+// list order — the JW sign depends only on (spin, from, to), so the operator is unchanged.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace ftlm_b200 {
+
+struct HopIn {
+  int from, to, spin;
+  double cre, cim;
+};
+struct PairIn {
+  int i, j;
+};
+
+uint64_t binom(int n, int k);
+
+struct SpinSpace {
+  int n = 0, k = 0;
+  int64_t D = 0;
+  std::vector<uint32_t> masks;  // lexicographic order
+  void build(int n_, int k_);
+  int64_t rank(uint32_t m) const;  // -1 if m is not a k-subset of the n sites
+};
+
+// One merged directed hop of one spin species.
+struct MergedHop {
+  int from, to;
+  double cre, cim;
+  uint32_t own_mask;    // sites of the same species strictly between lo and hi
+  uint32_t other_mask;  // sites of the other species counted by the JW sign
+  int lo, hi;
+};
+
+struct SectorPlan {
+  int n = 0, nu = 0, nd = 0;
+  double U = 0.0, V = 0.0;
+  SpinSpace up, dn;
+  std::vector<MergedHop> hu, hd;
+  std::vector<PairIn> pairs;
+  int64_t dim = 0;
+
+  // Diagonal: H_ii = U*popc(u&d) + V*(cnt_uu[ru] + cnt_dd[rd] + sum_b 2^b popc(d & wpl[ru][b])).
+  std::vector<int32_t> cnt_uu, cnt_dd;
+  std::vector<uint32_t> wpl;  // 4 per up string: bit-planes of #pair partners occupied by up
+
+  // Up part (gather CSR over output up ranks): sources, coefficient with the up-string JW
+  // factor folded in, and packed (lo | hi<<8) for the per-element down-string factor.
+  std::vector<int32_t> up_ptr, up_src;
+  std::vector<double> up_coef;  // 2 per entry
+  std::vector<uint32_t> up_lohi;
+
+  // Down part (ELL, 32 consecutive output down ranks per group, entry k of lane l at
+  // dn_gptr[g] + 32k + l): entry = src_rank<<10 | hop_id<<1 | dn_string_sign.  Padding
+  // entries carry hop_id == dn_pad_hop.  Per down hop: coefficient and the up-site mask of
+  // its per-row sign.
+  std::vector<int64_t> dn_gptr;
+  std::vector<uint32_t> dn_ent;
+  int dn_pad_hop = 0;
+  std::vector<double> dn_coef;     // 2 per hop id (pad hop id has 0)
+  std::vector<uint32_t> dn_nmask;  // per hop id
+
+  double mean_up_sources = 0.0, mean_dn_sources = 0.0;
+  int max_dn_deg = 0, max_up_deg = 0;
+};
+
+// Builds the plan; returns "" on success or an error message (reference argument errors:
+// src/fock_basis.cpp:19-24).
+std::string build_plan(int n_sites, int n_up, int n_dn, double U, double V, const std::vector<HopIn>& hops,
+                       const std::vector<PairIn>& pairs, SectorPlan* out);
+
+// Diagonal entry from the plan tables (host).
+double plan_diag(const SectorPlan& p, int64_t ru, int64_t rd);
+
+// build_hubbard_geometry (reference src/lattice.cpp:38-110), host.
+void build_geometry(int Lx, int Ly, double t, double tp, double phix, double phiy, std::vector<HopIn>* hops,
+                    std::vector<PairIn>* pairs);
+
+}  // namespace ftlm_b200

@@ -1,0 +1,143 @@
+/* ftlm_gpu.h — C ABI of the B200 FTLM hot path for the 2D extended Hubbard model.
+ *
+ * Every entry point returns an int status (FTLM_OK == 0).  No exception crosses this
+ * boundary; on failure ftlm_gpu_last_error() returns a message for the calling thread.
+ * Complex vectors are interleaved (re, im) doubles ("complex128") or floats
+ * ("complex64").  Functions taking *_dev pointers expect device memory on the current
+ * CUDA device; *_host pointers are ordinary host memory.  A `stream` argument is a
+ * cudaStream_t passed as void* (NULL = the legacy default stream).  Sector handles are
+ * not thread-safe: use one host thread per handle.
+ *
+ * Reference interfaces replaced (paths inside PeizhiMai/FTLM_extended_Hubbard):
+ *   ftlm_gpu_sector_create        FockBasis(n_sites,n_up,n_down)      include/ftlm/fock_basis.hpp:13
+ *                                 + build_hubbard_geometry            include/ftlm/lattice.hpp:38-40
+ *   ftlm_gpu_sector_create_hops   FockBasis + caller-supplied hoppings/nn_pairs
+ *                                 (the vectors apply_extended_hubbard takes)  include/ftlm/hubbard_hamiltonian.hpp:13-16
+ *   ftlm_gpu_sector_dim/masks/index_of   FockBasis::dim/up_mask/down_mask/index_of  include/ftlm/fock_basis.hpp:18-24
+ *   ftlm_gpu_apply / _apply_host  apply_extended_hubbard               include/ftlm/hubbard_hamiltonian.hpp:13-16
+ *   ftlm_gpu_lanczos              lanczos_tridiagonal                  include/ftlm/lanczos.hpp:55-59
+ *   ftlm_gpu_lanczos_extrema      lanczos_extrema                      include/ftlm/lanczos.hpp:45-48
+ *   ftlm_gpu_lanczos_op           lanczos_tridiagonal with a caller operator (std::function apply_h)
+ *   ftlm_gpu_tridiag_quadrature   log_lanczos_tridiagonal_quadrature_exp  src/ftlm_thermo.cpp:83-146
+ *   ftlm_gpu_ftlm_sector          ftlm_log_partition_complex/_real     include/ftlm/ftlm_thermo.hpp:41-50
+ *   ftlm_gpu_gc_reduce            grand-canonical mu loop              benchmarks/bench_ftlm_nmu_rect.cpp:186-219
+ *   ftlm_gpu_gc_sweep             sector loop + mu loop                benchmarks/bench_ftlm_nmu_rect.cpp:138-219
+ */
+#ifndef FTLM_GPU_H_
+#define FTLM_GPU_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FTLM_OK 0
+#define FTLM_ERR_INVALID 1     /* bad argument: the reference throws std::invalid_argument */
+#define FTLM_ERR_CUDA 2        /* CUDA runtime error (including "no device") */
+#define FTLM_ERR_NOMEM 3       /* device or host allocation failed */
+#define FTLM_ERR_TIMEOUT 4     /* a bounded device-side wait ran out */
+#define FTLM_ERR_UNSUPPORTED 5 /* outside the sizes this build supports */
+
+/* Mirrors ftlm::HubbardParams (include/ftlm/hubbard_params.hpp:6-15). */
+typedef struct ftlm_params {
+  int Lx, Ly;
+  double t, tp, U, V, phi_x, phi_y;
+} ftlm_params;
+
+/* Mirrors ftlm::SpinfulHopping (include/ftlm/lattice.hpp:11-16): H += coeff c^dag_to c_from. */
+typedef struct ftlm_hop {
+  int from, to, spin; /* spin 0 = up, 1 = down */
+  double coeff_re, coeff_im;
+} ftlm_hop;
+
+/* Mirrors ftlm::NearestPair (include/ftlm/lattice.hpp:19-22). */
+typedef struct ftlm_pair {
+  int i, j;
+} ftlm_pair;
+
+typedef struct ftlm_sector ftlm_sector;
+
+/* Start vectors of Lanczos chains. */
+#define FTLM_START_REFERENCE 0 /* std::mt19937(seed)+std::normal_distribution, host-made (src/lanczos.cpp:140-175) */
+#define FTLM_START_PHILOX 1    /* Philox4x32-10 + Box-Muller on the device (counter = element, key = seed) */
+
+const char* ftlm_gpu_last_error(void);
+const char* ftlm_gpu_version_string(void);
+int ftlm_gpu_device_count(int* n);
+
+/* Geometry exactly as build_hubbard_geometry (src/lattice.cpp:38-110); host-only, no GPU needed.
+ * Returns the hop count in *n_hops and pair count in *n_pairs; writes at most max_* entries. */
+int ftlm_gpu_build_geometry(const ftlm_params* p, ftlm_hop* hops, int max_hops, int* n_hops, ftlm_pair* pairs,
+                            int max_pairs, int* n_pairs);
+
+/* Sector = FockBasis(Lx*Ly, n_up, n_dn) + its device tables.  n_sites <= 32, each spin
+ * space <= 2^22 strings, dim = C(n,n_up)*C(n,n_dn) < 2^31 (the reference's int index). */
+int ftlm_gpu_sector_create(const ftlm_params* p, int n_up, int n_dn, ftlm_sector** out);
+int ftlm_gpu_sector_create_hops(int n_sites, int n_up, int n_dn, double U, double V, const ftlm_hop* hops, int n_hops,
+                                const ftlm_pair* pairs, int n_pairs, ftlm_sector** out);
+/* Host-only variant (no device tables): basis, tables and plan statistics for CPU checks. */
+int ftlm_gpu_sector_create_host(int n_sites, int n_up, int n_dn, double U, double V, const ftlm_hop* hops, int n_hops,
+                                const ftlm_pair* pairs, int n_pairs, ftlm_sector** out);
+int ftlm_gpu_sector_destroy(ftlm_sector* s);
+int ftlm_gpu_sector_dim(const ftlm_sector* s, long long* dim);
+int ftlm_gpu_sector_masks(const ftlm_sector* s, uint64_t* up_host, uint64_t* dn_host);
+int ftlm_gpu_sector_index_of(const ftlm_sector* s, uint64_t up, uint64_t dn, long long* index);
+/* Mean number of distinct up-hop source rows per up string (the row-gather traffic model). */
+int ftlm_gpu_sector_stats(const ftlm_sector* s, double* mean_up_sources, double* mean_dn_sources, long long* du,
+                          long long* dd);
+/* Diagonal entry H[i,i] (host computation from the sector tables). */
+int ftlm_gpu_sector_diag(const ftlm_sector* s, long long index, double* value);
+
+/* y = H x on device complex128 vectors of length dim (apply_extended_hubbard; y overwritten). */
+int ftlm_gpu_apply(ftlm_sector* s, const double* x_dev, double* y_dev, void* stream);
+/* Same with host buffers (copies in and out; the drop-in for apply_extended_hubbard). */
+int ftlm_gpu_apply_host(ftlm_sector* s, const double* x_host, double* y_host);
+/* Kernel selection for ftlm_gpu_apply: 0 = automatic, 1 = generic gather, 2 = row+slab passes. */
+int ftlm_gpu_set_apply_path(ftlm_sector* s, int path);
+
+/* lanczos_tridiagonal on the sector operator.  alpha/beta: host arrays of max_steps entries;
+ * *n_beta = number of beta entries written (steps used, or used-1 after a breakdown), *used =
+ * steps used.  start_mode: FTLM_START_REFERENCE or FTLM_START_PHILOX. */
+int ftlm_gpu_lanczos(ftlm_sector* s, int max_steps, unsigned seed, int start_mode, double* alpha, double* beta,
+                     int* n_beta, int* used);
+/* lanczos_extrema (min/max Ritz values with the reference's 120-rotation Jacobi). */
+int ftlm_gpu_lanczos_extrema(ftlm_sector* s, int max_steps, unsigned seed, int start_mode, double* min_eval,
+                             double* max_eval, int* steps_used);
+
+/* Lanczos with a caller operator on device buffers: apply(x_dev, y_dev, ctx) computes y = H x. */
+typedef void (*ftlm_apply_fn)(const double* x_dev, double* y_dev, void* ctx);
+int ftlm_gpu_lanczos_op(long long dim, ftlm_apply_fn apply, void* ctx, int max_steps, unsigned seed, int start_mode,
+                        double* alpha, double* beta, int* n_beta, int* used);
+
+/* Ritz values and first-row weights of n_chains tridiagonals (alpha/beta: [n_chains][ld]),
+ * by the reference's classical Jacobi with max_rot rotations (<=0: max(3000,120n)) and tol.
+ * lam/w0 outputs [n_chains][ld]; n[c] = size of chain c.  Host buffers. */
+int ftlm_gpu_tridiag_eig(const double* alpha, const double* beta, const int* n, int n_chains, int ld, int max_rot,
+                         double tol, double* lam, double* w0);
+/* log sum_k w_k exp(-bT lam_k) per chain and temperature: out [n_chains][n_bt]. */
+int ftlm_gpu_tridiag_quadrature(const double* alpha, const double* beta, const int* n, int n_chains, int ld,
+                                const double* bts, int n_bt, double* logq, double* energy);
+/* Exact Ritz values (Sturm bisection, ascending) of one tridiagonal: lowest k into ritz[k]. */
+int ftlm_gpu_ritz_values(const double* alpha, const double* beta, int n, int k, double* ritz);
+
+/* ln Tr_s e^{-bT H} of one sector at n_bt temperatures from R chains of M steps
+ * (seed_r = seed + r*100003, src/ftlm_thermo.cpp:234), plus the FTLM energy <H>_s. */
+int ftlm_gpu_ftlm_sector(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed, int start_mode,
+                         double* lnz, double* energy);
+
+/* Grand-canonical combination over sectors (host arrays): lnz_s/e_s [n_sec][n_bt], N_s [n_sec];
+ * outputs [n_bt][n_mu]: ln Z_GC, <n> per site, <E>. */
+int ftlm_gpu_gc_reduce(const double* lnz_s, const double* e_s, const int* N_s, int n_sec, const double* bts, int n_bt,
+                       const double* mus, int n_mu, int n_sites, double* lnz_gc, double* n_avg, double* e_avg);
+
+/* Full plain sweep over all (N_up, N_dn) sectors of p: per-sector ln Z_s/E_s [n_sec][n_bt]
+ * with sector order nu*(n+1)+nd (bench_ftlm_nmu_rect.cpp:62), then the GC grid. */
+int ftlm_gpu_gc_sweep(const ftlm_params* p, int R, int M, unsigned seed, int start_mode, const double* bts, int n_bt,
+                      const double* mus, int n_mu, double* lnz_s, double* e_s, double* lnz_gc, double* n_avg,
+                      double* e_avg);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FTLM_GPU_H_ */
