@@ -67,6 +67,7 @@ SIGNATURES = {
     "ftlm_gpu_sector_diag": [_vp, _ll, _pd],
     "ftlm_gpu_apply": [_vp, _vp, _vp, _vp],
     "ftlm_gpu_apply_host": [_vp, _vp, _vp],
+    "ftlm_gpu_apply_profiled": [_vp, _vp, _vp, _vp, C.POINTER(C.c_float), _pi],
     "ftlm_gpu_set_apply_path": [_vp, _i],
     "ftlm_gpu_lanczos": [_vp, _i, C.c_uint, _i, _vp, _vp, _pi, _pi],
     "ftlm_gpu_lanczos_extrema": [_vp, _i, C.c_uint, _i, _pd, _pd, _pi],

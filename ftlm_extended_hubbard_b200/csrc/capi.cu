@@ -402,6 +402,36 @@ int ftlm_gpu_apply(ftlm_sector* s, const double* x, double* y, void* stream) {
   return s->apply(reinterpret_cast<const double2*>(x), reinterpret_cast<double2*>(y), static_cast<cudaStream_t>(stream));
 }
 
+int ftlm_gpu_apply_profiled(ftlm_sector* s, const double* x, double* y, void* stream, float* ms_passes, int* n_passes) {
+  int rc = need_device(s);
+  if (rc) return rc;
+  if (!x || !y || !ms_passes || !n_passes) return fail(FTLM_ERR_INVALID, "null argument");
+  if (x == y) return fail(FTLM_ERR_INVALID, "x and y must not alias");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int path = s->effective_path();
+  cudaEvent_t ev[3];
+  for (auto& e : ev) CU_TRY(cudaEventCreate(&e));
+  CU_TRY(cudaEventRecord(ev[0], st));
+  if (path == 2) {
+    CU_TRY(hv_launch_pass(s->dev, reinterpret_cast<const double2*>(x), reinterpret_cast<double2*>(y), 0, st));
+    CU_TRY(cudaEventRecord(ev[1], st));
+    CU_TRY(hv_launch_pass(s->dev, reinterpret_cast<const double2*>(x), reinterpret_cast<double2*>(y), 1, st));
+  } else {
+    CU_TRY(hv_launch(s->dev, reinterpret_cast<const double2*>(x), reinterpret_cast<double2*>(y), path, st));
+    CU_TRY(cudaEventRecord(ev[1], st));
+  }
+  CU_TRY(cudaEventRecord(ev[2], st));
+  CU_TRY(cudaEventSynchronize(ev[2]));
+  CU_TRY(cudaEventElapsedTime(&ms_passes[0], ev[0], ev[1]));
+  *n_passes = 1;
+  if (path == 2) {
+    CU_TRY(cudaEventElapsedTime(&ms_passes[1], ev[1], ev[2]));
+    *n_passes = 2;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  return FTLM_OK;
+}
+
 int ftlm_gpu_apply_host(ftlm_sector* s, const double* x, double* y) {
   int rc = need_device(s);
   if (rc) return rc;

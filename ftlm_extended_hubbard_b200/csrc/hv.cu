@@ -192,15 +192,19 @@ bool hv_fast_path_ok(const DevSector& S, int max_up_deg) {
   return hv_rows_smem_bytes(S) <= 220 * 1024 && max_up_deg <= kMaxUpDeg && S.dim >= (1 << 16);
 }
 
-cudaError_t hv_launch(const DevSector& S, const double2* x, double2* y, int path, cudaStream_t st) {
-  if (S.dim <= 0) return cudaSuccess;
+void init_sm_count() {
   if (g_num_sms == 0) {
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
     if (g_num_sms <= 0) g_num_sms = 148;
   }
-  if (path == 2) {
+}
+
+cudaError_t hv_launch_pass(const DevSector& S, const double2* x, double2* y, int pass, cudaStream_t st) {
+  if (S.dim <= 0) return cudaSuccess;
+  init_sm_count();
+  if (pass == 0) {
     cudaError_t e = cudaMemsetAsync(S.flags, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
     const size_t sm = hv_rows_smem_bytes(S);
@@ -208,10 +212,21 @@ cudaError_t hv_launch(const DevSector& S, const double2* x, double2* y, int path
     if (e != cudaSuccess) return e;
     const int grid_r = static_cast<int>(std::min<int64_t>(S.Du, g_num_sms));
     hv_rows_kernel<<<grid_r, kRowThreads, sm, st>>>(S, x, y);
-    const int64_t nchunks = (S.Dd + kColThreads - 1) / kColThreads;
-    const int64_t grid_c = nchunks * S.Du;
-    hv_cols_kernel<<<static_cast<unsigned>(grid_c), kColThreads, 0, st>>>(S, x, y);
     return cudaGetLastError();
+  }
+  const int64_t nchunks = (S.Dd + kColThreads - 1) / kColThreads;
+  const int64_t grid_c = nchunks * S.Du;
+  hv_cols_kernel<<<static_cast<unsigned>(grid_c), kColThreads, 0, st>>>(S, x, y);
+  return cudaGetLastError();
+}
+
+cudaError_t hv_launch(const DevSector& S, const double2* x, double2* y, int path, cudaStream_t st) {
+  if (S.dim <= 0) return cudaSuccess;
+  init_sm_count();
+  if (path == 2) {
+    cudaError_t e = hv_launch_pass(S, x, y, 0, st);
+    if (e != cudaSuccess) return e;
+    return hv_launch_pass(S, x, y, 1, st);
   }
   const int64_t blocks = std::min<int64_t>((S.dim + 255) / 256, static_cast<int64_t>(g_num_sms) * 16);
   hv_generic_kernel<<<static_cast<unsigned>(blocks), 256, 0, st>>>(S, x, y);

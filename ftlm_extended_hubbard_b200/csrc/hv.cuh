@@ -9,6 +9,8 @@ namespace ftlm_b200 {
 
 // path: 1 = generic gather kernel, 2 = row pass + column-slab pass.
 cudaError_t hv_launch(const DevSector& S, const double2* x, double2* y, int path, cudaStream_t st);
+// One pass of the fast path: 0 = row pass (diag + down hops), 1 = column-slab pass (up hops).
+cudaError_t hv_launch_pass(const DevSector& S, const double2* x, double2* y, int pass, cudaStream_t st);
 bool hv_fast_path_ok(const DevSector& S, int max_up_deg);
 size_t hv_rows_smem_bytes(const DevSector& S);
 

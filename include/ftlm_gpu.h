@@ -93,6 +93,10 @@ int ftlm_gpu_sector_diag(const ftlm_sector* s, long long index, double* value);
 int ftlm_gpu_apply(ftlm_sector* s, const double* x_dev, double* y_dev, void* stream);
 /* Same with host buffers (copies in and out; the drop-in for apply_extended_hubbard). */
 int ftlm_gpu_apply_host(ftlm_sector* s, const double* x_host, double* y_host);
+/* ftlm_gpu_apply with CUDA-event timing of each kernel pass on `stream` (synchronises): ms_passes[0..1]
+ * = row pass, column-slab pass (one entry for the generic path); *n_passes = entries written. */
+int ftlm_gpu_apply_profiled(ftlm_sector* s, const double* x_dev, double* y_dev, void* stream, float* ms_passes,
+                            int* n_passes);
 /* Kernel selection for ftlm_gpu_apply: 0 = automatic, 1 = generic gather, 2 = row+slab passes. */
 int ftlm_gpu_set_apply_path(ftlm_sector* s, int path);
 

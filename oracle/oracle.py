@@ -85,8 +85,11 @@ def _load_ref() -> C.CDLL | None:
     L.ref_sector_index_of.restype = _i
     L.ref_sector_index_of.argtypes = [_vp, C.c_uint64, C.c_uint64]
     L.ref_sector_apply.argtypes = [_vp, _vp, _vp]
-    L.ref_sector_apply_sample.restype = _d
-    L.ref_sector_apply_sample.argtypes = [_vp, _ll, _ll, _i, C.POINTER(_ll)]
+    L.ref_sample_create.restype = _vp
+    L.ref_sample_create.argtypes = [_vp, _i]
+    L.ref_sample_destroy.argtypes = [_vp]
+    L.ref_sample_run.restype = _d
+    L.ref_sample_run.argtypes = [_vp, _ll, _ll, C.POINTER(_ll)]
     L.ref_sector_lanczos.restype = _i
     L.ref_sector_lanczos.argtypes = [_vp, _i, C.c_uint, _vp, _vp, C.POINTER(_i)]
     L.ref_sector_lanczos_extrema.restype = _i

@@ -130,35 +130,60 @@ void ref_sector_apply(void* h, const double* x, double* y) {
                                reinterpret_cast<cd*>(y));
 }
 
-// Timed CPU sample of the reference apply: `nthreads` threads each run apply_extended_hubbard
-// on their own x/y pair in which only `ncols` consecutive columns are non-zero (the reference
-// skips columns with |x|^2 < 1e-28), so each call processes exactly `ncols` columns plus its
-// fixed O(dim) fill/scan.  Returns wall seconds of the parallel region; *cols_done receives the
-// total number of processed columns.  x values are deterministic (not random): 1/sqrt(ncols).
-double ref_sector_apply_sample(void* h, long long col0, long long ncols, int nthreads, long long* cols_done) {
+// Timed CPU samples of the reference apply for a sector too large to apply in full on the CPU:
+// `nthreads` threads each own an x/y pair (allocated once) and call apply_extended_hubbard on an
+// x that is non-zero on `ncols` consecutive columns only.  The reference skips columns with
+// |x|^2 < 1e-28, so one call processes exactly `ncols` columns plus its fixed O(dim) fill of y
+// and scan of x.  ref_sample_run returns the wall seconds of the parallel region and the number
+// of processed columns.
+struct RefSample {
+  RefSector* s;
+  int nthreads;
+  std::vector<std::vector<cd>> xs, ys;
+  std::vector<long long> c0;
+  long long ncols_prev = 0;
+};
+
+void* ref_sample_create(void* h, int nthreads) {
   auto* s = static_cast<RefSector*>(h);
-  const long long dim = s->basis.dim();
   if (nthreads < 1) nthreads = 1;
-  std::vector<std::vector<cd>> xs(static_cast<size_t>(nthreads)), ys(static_cast<size_t>(nthreads));
-  for (int t = 0; t < nthreads; ++t) {
-    xs[t].assign(static_cast<size_t>(dim), cd(0.0, 0.0));
-    ys[t].assign(static_cast<size_t>(dim), cd(0.0, 0.0));
-    const long long c0 = (col0 + static_cast<long long>(t) * ncols) % dim;
-    for (long long c = 0; c < ncols; ++c) {
-      xs[t][static_cast<size_t>((c0 + c) % dim)] = cd(0.5, -0.25);
+  try {
+    auto* c = new RefSample{s, nthreads, {}, {}, {}, 0};
+    const size_t dim = static_cast<size_t>(s->basis.dim());
+    c->xs.resize(static_cast<size_t>(nthreads));
+    c->ys.resize(static_cast<size_t>(nthreads));
+    c->c0.assign(static_cast<size_t>(nthreads), 0);
+    for (int t = 0; t < nthreads; ++t) {
+      c->xs[t].assign(dim, cd(0.0, 0.0));
+      c->ys[t].assign(dim, cd(0.0, 0.0));
     }
+    return c;
+  } catch (...) {
+    return nullptr;
   }
+}
+
+void ref_sample_destroy(void* c) { delete static_cast<RefSample*>(c); }
+
+double ref_sample_run(void* ctx, long long col0, long long ncols, long long* cols_done) {
+  auto* c = static_cast<RefSample*>(ctx);
+  const long long dim = c->s->basis.dim();
+  for (int t = 0; t < c->nthreads; ++t) {
+    for (long long k = 0; k < c->ncols_prev; ++k) c->xs[t][static_cast<size_t>((c->c0[t] + k) % dim)] = cd(0.0, 0.0);
+    c->c0[t] = (col0 + static_cast<long long>(t) * ncols) % dim;
+    for (long long k = 0; k < ncols; ++k) c->xs[t][static_cast<size_t>((c->c0[t] + k) % dim)] = cd(0.5, -0.25);
+  }
+  c->ncols_prev = ncols;
   const auto t0 = std::chrono::steady_clock::now();
   std::vector<std::thread> th;
-  for (int t = 0; t < nthreads; ++t) {
-    th.emplace_back([&, t]() {
-      ftlm::apply_extended_hubbard(s->p, s->basis, s->hops, s->pairs, xs[t].data(), ys[t].data());
+  for (int t = 0; t < c->nthreads; ++t) {
+    th.emplace_back([c, t]() {
+      ftlm::apply_extended_hubbard(c->s->p, c->s->basis, c->s->hops, c->s->pairs, c->xs[t].data(), c->ys[t].data());
     });
   }
   for (auto& x : th) x.join();
-  const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  *cols_done = static_cast<long long>(nthreads) * ncols;
-  return sec;
+  *cols_done = static_cast<long long>(c->nthreads) * ncols;
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
 // lanczos_tridiagonal on this sector with the full complex apply.  alpha has room for M,

@@ -1,0 +1,158 @@
+"""Generates the golden fixtures under tests/golden/ (run where the reference sources exist):
+
+    python tests/golden/make_golden.py
+
+published_tsv.npz  the reference's own published n(mu) tables (benchmarks/data/*.tsv of
+                   PeizhiMai/FTLM_extended_Hubbard), parsed: 2x2 and 4x2 from bench_ftlm_nmu_rect,
+                   3x2 from the non-momentum solver; plus the per-sector ln Z lines of the 3x2 run log.
+ref_small.npz      outputs of the reference library itself (oracle/_ref): H·x on seeded vectors,
+                   Lanczos alpha/beta, lanczos_extrema, and sector ln Z for small sectors.
+config0_4x2.npz    the plain FTLM sweep of 4x2, t=1 t'=-0.25 U=8 V=1, phi=0, R=20, M=60, seed 7,
+                   T = 0.1..2.0 (20) x mu = -4..8 (49), computed by the oracle in the reference's
+                   scatter order (bit-identical to the reference library; this script checks the
+                   sector ln Z of several sectors against the reference itself before writing).
+"""
+from __future__ import annotations
+
+import os
+import re
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import oracle as O  # noqa: E402
+
+REF_DATA = os.path.join(O.REFERENCE_SRC, "benchmarks", "data")
+
+SMALL_CASES = [
+    # Lx, Ly, t, tp, U, V, phix, phiy, nu, nd
+    (2, 2, 1.0, 0.0, 0.0, 0.0, 0.31, -0.27, 2, 2),
+    (2, 1, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1, 1),
+    (3, 2, 1.0, -0.35, 5.75, 0.9, 0.0, 0.0, 2, 3),
+    (4, 2, 1.0, -0.25, 8.0, 1.0, 0.0, 0.0, 4, 4),
+    (4, 2, 1.0, -0.25, 8.0, 1.0, 0.0, 0.0, 3, 1),
+    (3, 3, 1.0, -0.35, 5.75, 0.9, 0.2, 0.1, 4, 5),
+    (4, 3, 1.0, -0.25, 8.0, 1.0, 0.1, 0.0, 3, 2),
+    (5, 1, 1.0, 0.3, 2.0, 0.5, 0.4, 0.0, 2, 3),
+    (1, 4, 1.0, 0.0, 3.0, 0.0, 0.0, 0.7, 2, 1),
+]
+
+
+def parse_tsv(path):
+    mu, n = [], []
+    hdr = []
+    with open(path) as f:
+        for line in f:
+            if line.startswith("#"):
+                hdr.append(line.strip())
+                continue
+            a, b = line.split()
+            mu.append(float(a))
+            n.append(float(b))
+    return np.array(mu), np.array(n), "\n".join(hdr)
+
+
+def published():
+    out = {}
+    for key, fn in [("2x2", "n_vs_mu_2x2_beta20_ftlm.tsv"), ("4x2", "n_vs_mu_4x2_beta20_ftlm.tsv"),
+                    ("3x2_nonmom", "n_vs_mu_3x2_beta20_solver_nonmom.tsv")]:
+        mu, n, hdr = parse_tsv(os.path.join(REF_DATA, fn))
+        out[f"{key}_mu"] = mu
+        out[f"{key}_n"] = n
+        out[f"{key}_header"] = np.array(hdr)
+    # per-sector ln Z printed by the 3x2 non-momentum run (6 significant digits)
+    sec, lz = [], []
+    with open(os.path.join(REF_DATA, "n_vs_mu_3x2_beta20_four_solver_monitoring.txt")) as f:
+        in_block = False
+        for line in f:
+            if "solver=nonmom" in line:
+                in_block = True
+            elif in_block and line.startswith("---"):
+                break
+            m = re.match(r"sector \((\d+),(\d+)\) dim=(\d+) logZ=(\S+)", line.strip())
+            if in_block and m:
+                sec.append((int(m.group(1)), int(m.group(2)), int(m.group(3))))
+                lz.append(float(m.group(4)))
+    out["3x2_sector"] = np.array(sec, np.int64)
+    out["3x2_sector_lnz"] = np.array(lz)
+    return out
+
+
+def ref_small():
+    R = O.reference()
+    assert R is not None, "reference library unavailable"
+    out = {"cases": np.array(SMALL_CASES, dtype=np.float64)}
+    rng = np.random.default_rng(20240601)
+    import ctypes as C
+    for k, c in enumerate(SMALL_CASES):
+        h = R.ref_sector_create(*c)
+        dim = R.ref_sector_dim(h)
+        x = rng.standard_normal(dim) + 1j * rng.standard_normal(dim)
+        x[rng.random(dim) < 0.05] = 0.0  # zero columns exercise the skip rule
+        y = np.zeros(dim, np.complex128)
+        R.ref_sector_apply(h, O.P(x), O.P(y))
+        M = 40
+        a = np.zeros(M)
+        b = np.zeros(M)
+        nb = C.c_int()
+        used = R.ref_sector_lanczos(h, M, 11 + k, O.P(a), O.P(b), C.byref(nb))
+        mn, mx = C.c_double(), C.c_double()
+        ue = R.ref_sector_lanczos_extrema(h, 30, 5, C.byref(mn), C.byref(mx))
+        lz = R.ref_sector_ftlm_complex(h, 2.0, 6, 30, 3)
+        up = np.zeros(dim, np.uint64)
+        dn = np.zeros(dim, np.uint64)
+        R.ref_sector_masks(h, O.P(up), O.P(dn))
+        out[f"x{k}"] = x
+        out[f"y{k}"] = y
+        out[f"up{k}"] = up
+        out[f"dn{k}"] = dn
+        out[f"alpha{k}"] = a[:used]
+        out[f"beta{k}"] = b[:nb.value]
+        out[f"extrema{k}"] = np.array([mn.value, mx.value, ue])
+        out[f"lnz{k}"] = np.array([lz])
+        R.ref_sector_destroy(h)
+    # tests/test_ftlm_thermo.cpp known answer: diag(2,3), beta=1, R=48, M=32, seed 12345
+    d = np.array([2.0, 3.0])
+    out["diag23_lnz"] = np.array([R.ref_ftlm_diag_real(O.P(d), 2, 1.0, 48, 32, 12345)])
+    return out
+
+
+CONFIG0 = dict(Lx=4, Ly=2, t=1.0, tp=-0.25, U=8.0, V=1.0, phix=0.0, phiy=0.0, R=20, M=60, seed=7)
+T_GRID = np.round(np.arange(1, 21) * 0.1, 10)
+MU_GRID = np.round(np.arange(49) * 0.25 - 4.0, 10)
+
+
+def config0():
+    c = CONFIG0
+    betas = 1.0 / T_GRID
+    lz, es, N, dims, (g_lnz, g_n, g_e) = O.oracle_sweep(c["Lx"], c["Ly"], c["t"], c["tp"], c["U"], c["V"], c["phix"],
+                                                       c["phiy"], c["R"], c["M"], c["seed"], betas, MU_GRID, mode=0)
+    # Pin against the reference library on sectors spanning small to largest, two temperatures.
+    R = O.reference()
+    n = c["Lx"] * c["Ly"]
+    for nu, nd in [(0, 1), (1, 1), (2, 3), (4, 4), (8, 8), (3, 5)]:
+        idx = nu * (n + 1) + nd
+        h = R.ref_sector_create(c["Lx"], c["Ly"], c["t"], c["tp"], c["U"], c["V"], c["phix"], c["phiy"], nu, nd)
+        for bi in (0, 9):
+            ref = R.ref_sector_ftlm_real(h, float(betas[bi]), c["R"], c["M"], c["seed"])
+            assert ref == lz[idx, bi], (nu, nd, bi, ref, lz[idx, bi])
+        R.ref_sector_destroy(h)
+    return {"lnz_sector": lz, "e_sector": es, "N": N, "dims": dims, "T": T_GRID, "mu": MU_GRID,
+            "lnz_gc": g_lnz, "n_gc": g_n, "e_gc": g_e,
+            "params": np.array([c["Lx"], c["Ly"], c["t"], c["tp"], c["U"], c["V"], c["phix"], c["phiy"], c["R"],
+                                c["M"], c["seed"]], dtype=np.float64)}
+
+
+def main():
+    O.build(ref=True)
+    np.savez_compressed(os.path.join(HERE, "published_tsv.npz"), **published())
+    np.savez_compressed(os.path.join(HERE, "ref_small.npz"), **ref_small())
+    np.savez_compressed(os.path.join(HERE, "config0_4x2.npz"), **config0())
+    print("wrote", os.listdir(HERE))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,305 @@
+"""GPU parity of the C ABI (ftlm_gpu_*) against the reference-pinned oracle and the golden vectors.
+
+Tolerances: integer work (basis, ranks, hop pattern and signs) bit-exact; H·v values within
+1e-13 relative (different summation order, FMA); Lanczos alpha/beta of the first steps within
+1e-12 and ln Z / <n> / <E> / converged Ritz values within 1e-10 relative (the bar the FTLM path
+states); Jacobi eigenpairs within 1e-12.
+"""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+import oracle as O
+import ftlm_extended_hubbard_b200 as F
+from ftlm_extended_hubbard_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+RTOL_HV = 1e-13
+RTOL_THERMO = 1e-10
+
+
+def relerr(a, b):
+    return float(np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-300))
+
+
+def sector_of(c):
+    Lx, Ly, t, tp, U, V, px, py, nu, nd = c
+    return F.Sector(F.HubbardParams(int(Lx), int(Ly), t, tp, U, V, px, py), int(nu), int(nd))
+
+
+def case_tuple(c):
+    return tuple(int(v) if i in (0, 1, 8, 9) else float(v) for i, v in enumerate(c))
+
+
+def test_apply_matches_reference_golden(gpu, golden):
+    g = golden("ref_small.npz")
+    for k, c in enumerate(g["cases"]):
+        c = case_tuple(c)
+        s = sector_of(c)
+        up, dn = s.masks()
+        assert np.array_equal(up, g[f"up{k}"]) and np.array_equal(dn, g[f"dn{k}"])
+        for path in (1, 2):
+            s.set_apply_path(path)
+            if path == 2 and s.dim() < 64:
+                continue
+            try:
+                y = s.apply_host(g[f"x{k}"])
+            except F.FtlmError as e:
+                assert path == 2 and e.code == _lib.FTLM_ERR_UNSUPPORTED
+                continue
+            assert relerr(y, g[f"y{k}"]) < RTOL_HV, (c, path)
+
+
+@pytest.mark.parametrize("c", [(2, 2, 1.0, 0.0, 0.0, 0.0, 0.31, -0.27, 2, 2), (3, 2, 1.0, -0.35, 5.75, 0.9, 0.0, 0.0, 2, 3),
+                               (4, 2, 1.0, -0.25, 8.0, 1.0, 0.3, -0.2, 3, 2), (1, 5, 1.0, 0.4, 2.0, 1.5, 0.0, 0.5, 2, 2),
+                               (3, 3, 1.0, -0.25, 8.0, 1.0, 0.1, 0.0, 2, 1)])
+def test_matrix_elements_exact(gpu, c):
+    """Dense H from e_j columns: the sparsity pattern and every off-diagonal element (hop
+    coefficient x JW sign) bit-exact against the reference-order oracle; diagonal within 4 ulp."""
+    s = sector_of(c)
+    o = O.OracleSector(*c)
+    dim = s.dim()
+    Hg = np.zeros((dim, dim), np.complex128)
+    Ho = np.zeros((dim, dim), np.complex128)
+    e = np.zeros(dim, np.complex128)
+    for j in range(dim):
+        e[:] = 0
+        e[j] = 1.0
+        Hg[:, j] = s.apply_host(e)
+        Ho[:, j] = o.apply(e, mode=0)
+    off = ~np.eye(dim, dtype=bool)
+    assert np.array_equal(Hg != 0, Ho != 0)
+    assert np.array_equal(Hg[off], Ho[off])
+    d = np.diag(Ho).real
+    assert np.all(np.abs(np.diag(Hg).real - d) <= 4 * np.spacing(np.maximum(np.abs(d), 1.0)))
+    assert np.abs(Hg - Hg.conj().T).max() <= 1e-14 * max(1.0, np.abs(Hg).max())  # Hermitian
+
+
+@pytest.mark.parametrize("c", [(4, 4, 1.0, -0.25, 8.0, 1.0, 0.1, 0.0, 4, 4), (4, 4, 1.0, -0.25, 8.0, 1.0, 0.1, 0.0, 8, 1),
+                               (4, 3, 1.0, -0.2, 4.0, 1.0, 0.0, 0.0, 6, 6), (4, 4, 1.0, 0.3, 2.0, 0.5, 0.2, -0.4, 5, 7)])
+def test_paths_agree_and_match_oracle(gpu, c):
+    s = sector_of(c)
+    o = O.OracleSector(*c)
+    dim = s.dim()
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal(dim) + 1j * rng.standard_normal(dim)
+    x[rng.random(dim) < 0.02] = 0.0
+    ys = []
+    for path in (1, 2):
+        s.set_apply_path(path)
+        ys.append(s.apply_host(x))
+    assert np.array_equal(ys[0], ys[1])  # same summation order in both paths
+    yo = o.apply(x, mode=1, nthreads=8)
+    assert relerr(ys[1], yo) < RTOL_HV
+
+
+def test_tiny_entries_follow_reference_skip_rule(gpu):
+    """Sources with |x|^2 < 1e-28 contribute nothing (src/hubbard_hamiltonian.cpp:62), on both paths."""
+    c = (4, 4, 1.0, -0.25, 8.0, 1.0, 0.1, 0.0, 4, 4)
+    s = sector_of(c)
+    o = O.OracleSector(*c)
+    dim = s.dim()
+    rng = np.random.default_rng(8)
+    x = rng.standard_normal(dim) + 1j * rng.standard_normal(dim)
+    x[rng.random(dim) < 0.2] = 3e-15 - 2e-15j
+    yo = o.apply(x, mode=1, nthreads=8)
+    for path in (1, 2):
+        s.set_apply_path(path)
+        y = s.apply_host(x)
+        assert relerr(y, yo) < RTOL_HV
+    # and a vector made only of tiny entries maps to exactly zero
+    t = np.full(dim, 1e-15 + 0j)
+    for path in (1, 2):
+        s.set_apply_path(path)
+        assert not np.any(s.apply_host(t))
+
+
+def test_large_sector_properties(gpu):
+    """4x4 (8,8), dim 165,636,900: oracle rows, Hermiticity and linearity at full size."""
+    torch = gpu
+    c = (4, 4, 1.0, -0.25, 8.0, 1.0, 0.1, 0.0, 8, 8)
+    s = sector_of(c)
+    dim = s.dim()
+    assert dim == math.comb(16, 8) ** 2
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1)
+    a = torch.randn(dim, dtype=torch.complex128, device="cuda", generator=g)
+    b = torch.randn(dim, dtype=torch.complex128, device="cuda", generator=g)
+    ha = torch.empty_like(a)
+    hb = torch.empty_like(a)
+    s.apply(a, ha)
+    s.apply(b, hb)
+    lhs = torch.vdot(a, hb).item()
+    rhs = torch.vdot(b, ha).item().conjugate()
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+    # linearity: H(a + 2i b) = Ha + 2i Hb
+    z = a + 2j * b
+    hz = torch.empty_like(z)
+    s.apply(z, hz)
+    err = (hz - (ha + 2j * hb)).abs().max().item()
+    assert err <= 1e-13 * hz.abs().max().item()
+    del z, hz, hb, b
+    # rows against the oracle
+    o = O.OracleSector(*c)
+    xh = a.cpu().numpy()
+    yh = ha.cpu().numpy()
+    yo = np.zeros(dim, np.complex128)
+    for r0 in (0, dim // 2 + 12345, dim - 30000):
+        o.L.or_sector_apply_rows(o.h, O.P(xh), O.P(yo), r0, r0 + 30000, 8)
+        assert relerr(yh[r0:r0 + 30000], yo[r0:r0 + 30000]) < RTOL_HV
+
+
+def test_lanczos_matches_reference_golden(gpu, golden):
+    g = golden("ref_small.npz")
+    for k, c in enumerate(g["cases"]):
+        c = case_tuple(c)
+        s = sector_of(c)
+        a, b, used = s.lanczos(40, 11 + k)
+        ar, br = g[f"alpha{k}"], g[f"beta{k}"]
+        if used != ar.size:
+            # The reference stops when ||w||^2 < 1e-24 (src/lanczos.cpp:187).  When the Krylov space is
+            # exhausted that quantity is rounding noise (~1e-25 here), so either side of the threshold is
+            # the same breakdown: the other run must show a noise-level beta at that step.
+            m = min(used, ar.size)
+            assert used > m and b[m - 1] < 1e-10, (c, used, ar.size)
+        m = min(used, ar.size)
+        k8 = min(8, m)
+        assert np.all(np.abs(a[:k8] - ar[:k8]) <= 1e-12 * np.maximum(1.0, np.abs(ar[:k8])))
+        # converged extremal Ritz value of the common chain
+        if m >= 2:
+            r1 = F.ritz_values(a[:m], b[:m - 1], 1)
+            r2 = F.ritz_values(ar[:m], br[:m - 1], 1)
+            assert abs(r1[0] - r2[0]) <= RTOL_THERMO * max(1.0, abs(r2[0]))
+
+
+def test_ftlm_sector_matches_reference_golden(gpu, golden):
+    g = golden("ref_small.npz")
+    for k, c in enumerate(g["cases"]):
+        c = case_tuple(c)
+        s = sector_of(c)
+        lz, _ = s.ftlm(2.0, 6, 30, 3)
+        assert abs(lz[0] - g[f"lnz{k}"][0]) <= RTOL_THERMO * max(1.0, abs(g[f"lnz{k}"][0])), c
+
+
+def test_lanczos_extrema_matches_reference_golden(gpu, golden):
+    g = golden("ref_small.npz")
+    for k, c in enumerate(g["cases"]):
+        c = case_tuple(c)
+        s = sector_of(c)
+        e = s.lanczos_extrema(30, 5)
+        mn, mx, ue = g[f"extrema{k}"]
+        assert e.steps_used == int(ue)
+        # 120-rotation Jacobi of the reference: same rotation sequence on nearly identical T
+        assert abs(e.min_eval - mn) <= 1e-9 * max(1.0, abs(mn)) and abs(e.max_eval - mx) <= 1e-9 * max(1.0, abs(mx))
+
+
+def test_config0_plain_sweep_matches_golden(gpu, golden):
+    """4x2, t'=-0.25, U=8, V=1: all 81 sectors, R=20, M=60, seed 7; ln Z, <n>, <E> on 20 T x 49 mu."""
+    g = golden("config0_4x2.npz")
+    p = F.HubbardParams(4, 2, 1.0, -0.25, 8.0, 1.0, 0.0, 0.0)
+    r = F.grand_canonical_sweep(p, 20, 60, 7, g["T"], g["mu"])
+    assert relerr(r.lnz_sector, g["lnz_sector"]) < RTOL_THERMO
+    assert relerr(r.e_sector, g["e_sector"]) < RTOL_THERMO
+    assert relerr(r.lnz_gc, g["lnz_gc"]) < RTOL_THERMO
+    assert relerr(r.n_avg, g["n_gc"]) < RTOL_THERMO
+    assert relerr(r.e_avg, g["e_gc"]) < RTOL_THERMO
+
+
+def test_jacobi_matches_oracle(gpu):
+    rng = np.random.default_rng(11)
+    sizes = [1, 2, 3, 7, 30, 60, 100]
+    ld = max(sizes)
+    A = np.zeros((len(sizes), ld))
+    B = np.zeros((len(sizes), ld))
+    for i, n in enumerate(sizes):
+        A[i, :n] = rng.standard_normal(n) * 5
+        B[i, :n] = np.abs(rng.standard_normal(n)) + 0.1
+    lam, w = F.tridiag_eig(A, B, np.array(sizes))
+    for i, n in enumerate(sizes):
+        l2, w2, rot, off = O.tridiag_eig(A[i, :n], B[i, :n])
+        scale = max(1.0, np.abs(l2).max())
+        assert np.abs(lam[i, :n] - l2).max() <= 1e-12 * scale
+        assert np.abs(w[i, :n] - w2).max() <= 1e-12
+
+
+def test_ritz_values_bisection(gpu):
+    rng = np.random.default_rng(2)
+    for n in (1, 2, 5, 40, 150):
+        a = rng.standard_normal(n)
+        b = rng.standard_normal(max(n - 1, 1))[: n - 1]
+        T = np.diag(a) + np.diag(b, 1) + np.diag(b, -1)
+        ev = np.linalg.eigvalsh(T)
+        r = F.ritz_values(a, b if n > 1 else np.zeros(1), 5)
+        assert np.abs(r - ev[: r.size]).max() <= 1e-12 * max(1.0, np.abs(ev).max())
+
+
+def test_known_answer_diag23_with_caller_operator(gpu, golden):
+    """tests/test_ftlm_thermo.cpp through the callback Lanczos: diag(2,3), beta=1, R=48, M=32, seed 12345."""
+    torch = gpu
+    d = torch.tensor([2.0, 3.0], dtype=torch.float64, device="cuda")
+    cudart = None
+    for name in ("libcudart.so.12", "/usr/local/cuda/lib64/libcudart.so.12", "/usr/local/cuda/lib64/libcudart.so"):
+        try:
+            cudart = C.CDLL(name)
+            break
+        except OSError:
+            continue
+    assert cudart is not None
+    cudart.cudaMemcpy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
+    cudart.cudaMemcpy.restype = C.c_int
+
+    def apply_h(xp, yp):
+        # y = diag(2,3) x on the device buffers handed over by the C ABI (device-to-device copies)
+        x = torch.empty(4, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        assert cudart.cudaMemcpy(x.data_ptr(), xp, 32, 3) == 0
+        y = (x.view(2, 2) * d[:, None]).reshape(4).contiguous()
+        torch.cuda.synchronize()
+        assert cudart.cudaMemcpy(yp, y.data_ptr(), 32, 3) == 0
+
+    est = F.ftlm_log_partition_complex(2, apply_h, 1.0, F.FtlmParams(48, 32, 12345))
+    exact = math.log(math.exp(-2.0) + math.exp(-3.0))
+    assert abs(est - exact) < 0.15
+    assert abs(est - golden("ref_small.npz")["diag23_lnz"][0]) <= RTOL_THERMO * abs(exact)
+
+
+def test_edge_sectors(gpu):
+    p = F.HubbardParams(3, 2, 1.0, -0.35, 5.75, 0.9, 0.2, 0.0)
+    for nu, nd in [(0, 0), (6, 6), (0, 6), (6, 0), (1, 0), (0, 1), (5, 6)]:
+        s = F.Sector(p, nu, nd)
+        o = O.OracleSector(3, 2, 1.0, -0.35, 5.75, 0.9, 0.2, 0.0, nu, nd)
+        x = np.arange(1, s.dim() + 1) * (1 + 0.5j)
+        assert relerr(s.apply_host(x), o.apply(x)) < RTOL_HV or not np.any(o.apply(x))
+        lz, _ = s.ftlm([1.0, 5.0], 4, 10, 7)
+        lzo, _ = o.ftlm([1.0, 5.0], 4, 10, 7)
+        assert np.all(np.abs(lz - lzo) <= RTOL_THERMO * np.maximum(1.0, np.abs(lzo)))
+    # one-site lattice: no hops, no pairs
+    s = F.Sector(F.HubbardParams(1, 1, 1.0, 0.0, 4.0, 1.0), 1, 1)
+    assert s.apply_host(np.array([2.0 + 1j]))[0] == 4.0 * (2.0 + 1j)
+
+
+def test_error_paths(gpu):
+    torch = gpu
+    s = F.Sector(F.HubbardParams(2, 2, 1.0), 1, 1)
+    x = torch.zeros(s.dim(), dtype=torch.complex128, device="cuda")
+    with pytest.raises(F.FtlmError) as e:
+        s.apply(x, x)
+    assert e.value.code == _lib.FTLM_ERR_INVALID
+    b = F.FockBasis(4, 2, 2)
+    with pytest.raises(F.FtlmError):
+        _lib.call("ftlm_gpu_apply", b.handle, C.c_void_p(x.data_ptr()), C.c_void_p(x.data_ptr() + 16), None)
+    with pytest.raises(F.FtlmError) as e:
+        s.ftlm(1.0, 2, 161, 1)
+    assert e.value.code == _lib.FTLM_ERR_UNSUPPORTED
+
+
+def test_philox_start_deterministic(gpu):
+    s = F.Sector(F.HubbardParams(4, 3, 1.0, -0.25, 8.0, 1.0), 3, 3)
+    a1, b1, _ = s.lanczos(12, 42, start="philox")
+    a2, b2, _ = s.lanczos(12, 42, start="philox")
+    a3, _, _ = s.lanczos(12, 43, start="philox")
+    assert np.array_equal(a1, a2) and np.array_equal(b1, b2)
+    assert not np.array_equal(a1, a3)

@@ -1,0 +1,135 @@
+"""Host-side logic of the native library (no GPU calls): exported C ABI, basis ranking, geometry,
+diagonal tables, plan statistics, and the reference's argument errors."""
+import ctypes as C
+import math
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle as O
+import ftlm_extended_hubbard_b200 as F
+from ftlm_extended_hubbard_b200 import _lib
+from conftest import ROOT, has_gpu
+
+
+def declared_symbols():
+    with open(os.path.join(ROOT, "include", "ftlm_gpu.h")) as f:
+        txt = f.read()
+    return sorted(set(re.findall(r"\b(ftlm_gpu_\w+)\s*\(", txt)))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    L = _lib.lib()
+    syms = declared_symbols()
+    assert len(syms) >= 20
+    for s in syms:
+        assert hasattr(L, s), s
+    assert set(syms) <= set(_lib.SIGNATURES), set(syms) - set(_lib.SIGNATURES)
+    assert "sm_100a" in F.version_string()
+
+
+@pytest.mark.parametrize("n,k", [(1, 0), (1, 1), (4, 2), (8, 4), (12, 6), (16, 8), (16, 3), (20, 10), (24, 2)])
+def test_rank_closed_form_matches_enumeration(n, k):
+    b = F.FockBasis(n, k, 0)
+    assert b.dim() == math.comb(n, k)
+    ref = np.zeros(math.comb(n, k), np.uint64)
+    assert O.oracle().or_enumerate(n, k, O.P(ref)) == ref.size
+    up, dn = b.masks()
+    assert np.array_equal(up, ref)
+    assert (dn == 0).all()
+    idx = [b.index_of(int(m), 0) for m in ref[:: max(1, ref.size // 2000)]]
+    assert idx == list(range(0, ref.size, max(1, ref.size // 2000)))
+
+
+@pytest.mark.parametrize("c", [(4, 2, 4, 4), (3, 3, 4, 5), (4, 3, 2, 3), (2, 2, 0, 4), (1, 1, 1, 0)])
+def test_fock_basis_matches_oracle(c):
+    Lx, Ly, nu, nd = c
+    b = F.FockBasis(Lx * Ly, nu, nd)
+    s = O.OracleSector(Lx, Ly, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, nu, nd)
+    up, dn = b.masks()
+    u2, d2 = s.masks()
+    assert np.array_equal(up, u2) and np.array_equal(dn, d2)
+    for i in range(0, b.dim(), max(1, b.dim() // 97)):
+        assert b.index_of(int(up[i]), int(dn[i])) == i == s.L.or_sector_index_of(s.h, int(up[i]), int(dn[i]))
+        assert b.up_mask(i) == int(up[i]) and b.down_mask(i) == int(dn[i])
+    # outside the sector -> -1 (FockBasis::index_of)
+    assert b.index_of(int(up[0]) ^ 1, int(dn[0])) == -1 or nu == 0 or nu == Lx * Ly
+    assert b.index_of(1 << 40, 0) == -1
+
+
+@pytest.mark.parametrize("lat", [(4, 4, 0.1, 0.0), (4, 2, 0.0, 0.0), (3, 3, 0.2, -0.3), (2, 2, 0.31, -0.27),
+                                 (1, 4, 0.0, 0.7), (1, 1, 0.0, 0.0)])
+def test_geometry_matches_oracle_bit_exact(lat):
+    Lx, Ly, px, py = lat
+    hops, pairs = F.build_hubbard_geometry(F.HubbardParams(Lx, Ly, 1.0, -0.25, 8.0, 1.0, px, py))
+    f = np.zeros(1024, np.int32)
+    t = np.zeros(1024, np.int32)
+    s = np.zeros(1024, np.int32)
+    cf = np.zeros(2048)
+    pi = np.zeros(256, np.int32)
+    pj = np.zeros(256, np.int32)
+    npair = C.c_int()
+    nh = O.oracle().or_geometry(Lx, Ly, 1.0, -0.25, px, py, 1024, O.P(f), O.P(t), O.P(s), O.P(cf), 256, O.P(pi),
+                                O.P(pj), C.byref(npair))
+    assert nh == len(hops) and npair.value == len(pairs)
+    for k, h in enumerate(hops):
+        assert (h.from_, h.to, h.spin) == (f[k], t[k], s[k])
+        assert h.coeff.real == cf[2 * k] and h.coeff.imag == cf[2 * k + 1]
+    assert [(p.i, p.j) for p in pairs] == list(zip(pi[:npair.value], pj[:npair.value]))
+
+
+def test_4x4_counts_from_survey():
+    """4x4: 384 directed hops (192 per spin), 32 NN pairs; mean distinct up-hop sources 34.133 at N=8."""
+    hops, pairs = F.build_hubbard_geometry(F.HubbardParams(4, 4, 1.0, -0.25, 8.0, 1.0, 0.1, 0.0))
+    assert len(hops) == 384 and len(pairs) == 32
+    h = C.c_void_p()
+    ch = F.api._c_hops(hops)
+    cp = F.api._c_pairs(pairs)
+    _lib.call("ftlm_gpu_sector_create_host", 16, 8, 8, 8.0, 1.0, ch, len(hops), cp, len(pairs), C.byref(h))
+    mu, md = C.c_double(), C.c_double()
+    du, dd = C.c_longlong(), C.c_longlong()
+    _lib.call("ftlm_gpu_sector_stats", h, C.byref(mu), C.byref(md), C.byref(du), C.byref(dd))
+    assert du.value == dd.value == 12870
+    assert abs(mu.value - 34.1333333333) < 1e-6 and abs(md.value - 34.1333333333) < 1e-6
+    _lib.lib().ftlm_gpu_sector_destroy(h)
+
+
+@pytest.mark.parametrize("c", [(4, 2, 1.0, -0.25, 8.0, 1.0, 0.0, 0.0, 4, 4), (3, 3, 1.0, -0.35, 5.75, 0.9, 0.2, 0.1, 4, 5),
+                               (2, 2, 1.0, 0.0, 3.0, 0.7, 0.0, 0.0, 2, 1)])
+def test_diagonal_tables_match_oracle(c):
+    Lx, Ly, t, tp, U, V, px, py, nu, nd = c
+    hops, pairs = F.build_hubbard_geometry(F.HubbardParams(Lx, Ly, t, tp, U, V, px, py))
+    h = C.c_void_p()
+    _lib.call("ftlm_gpu_sector_create_host", Lx * Ly, nu, nd, U, V, F.api._c_hops(hops), len(hops),
+              F.api._c_pairs(pairs), len(pairs), C.byref(h))
+    s = O.OracleSector(*c)
+    up, dn = s.masks()
+    v = C.c_double()
+    for i in range(0, s.dim, max(1, s.dim // 500)):
+        _lib.call("ftlm_gpu_sector_diag", h, i, C.byref(v))
+        ref = s.L.or_sector_diag(s.h, int(up[i]), int(dn[i]))
+        assert abs(v.value - ref) <= 4e-16 * max(1.0, abs(ref))
+    _lib.lib().ftlm_gpu_sector_destroy(h)
+
+
+def test_argument_errors_follow_reference():
+    with pytest.raises(ValueError):
+        F.FockBasis(0, 0, 0)
+    with pytest.raises(ValueError):
+        F.FockBasis(33, 1, 1)
+    with pytest.raises(ValueError):
+        F.FockBasis(4, 5, 0)
+    with pytest.raises(ValueError):
+        F.FockBasis(4, -1, 0)
+    with pytest.raises(F.FtlmError) as e:  # dim >= 2^31 is outside the reference's int index
+        F.FockBasis(20, 10, 10)
+    assert e.value.code == _lib.FTLM_ERR_UNSUPPORTED
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-device error path")
+def test_device_calls_fail_cleanly_without_gpu():
+    with pytest.raises(F.FtlmError) as e:
+        F.Sector(F.HubbardParams(2, 2, 1.0), 1, 1)
+    assert e.value.code in (_lib.FTLM_ERR_CUDA, _lib.FTLM_ERR_NOMEM)
