@@ -63,8 +63,12 @@ SIGNATURES = {
     "ftlm_gpu_sector_dim": [_vp, C.POINTER(_ll)],
     "ftlm_gpu_sector_masks": [_vp, _vp, _vp],
     "ftlm_gpu_sector_index_of": [_vp, C.c_uint64, C.c_uint64, C.POINTER(_ll)],
+    "ftlm_gpu_sector_state": [_vp, _ll, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
+    "ftlm_gpu_lanczos_host_op": [_ll, _vp, _vp, _i, C.c_uint, _i, _vp, _vp, _pi, _pi],
+    "ftlm_gpu_ftlm_combine": [_vp, _vp, _vp, _i, _i, _d, _vp, _vp],
     "ftlm_gpu_sector_stats": [_vp, _pd, _pd, C.POINTER(_ll), C.POINTER(_ll)],
     "ftlm_gpu_sector_diag": [_vp, _ll, _pd],
+    "ftlm_gpu_sector_down_table": [_vp, C.POINTER(_ll), C.POINTER(_ll), _vp, _vp, _pi],
     "ftlm_gpu_apply": [_vp, _vp, _vp, _vp],
     "ftlm_gpu_apply_host": [_vp, _vp, _vp],
     "ftlm_gpu_apply_profiled": [_vp, _vp, _vp, _vp, C.POINTER(C.c_float), _pi],

@@ -18,6 +18,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libftlm_gpu.so")
+DROPIN_LIB = os.path.join(HERE, "libftlm_dropin.so")
+DROPIN_SRC = os.path.join(HERE, "cpp", "dropin.cpp")
+DROPIN_INC = os.path.join(HERE, "cpp", "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"] + ARCH
@@ -78,6 +81,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
             list(ex.map(_run, jobs))
     if force or jobs or _stale(LIB, objs):
         _run([nvcc, "-shared", *ARCH, "-o", LIB, *objs, "-lcudart"])
+    # C++ drop-in of the reference API (namespace ftlm), host code over the C ABI
+    dhdrs = [os.path.join(DROPIN_INC, "ftlm", f) for f in os.listdir(os.path.join(DROPIN_INC, "ftlm"))]
+    if force or _stale(DROPIN_LIB, [DROPIN_SRC, LIB, os.path.join(ROOT, "include", "ftlm_gpu.h")] + dhdrs):
+        _run([cxx, *CXX_FLAGS, "-shared", "-I", DROPIN_INC, "-I", os.path.join(ROOT, "include"), DROPIN_SRC, "-o",
+              DROPIN_LIB, "-L", HERE, "-lftlm_gpu", "-Wl,-rpath,$ORIGIN"])
     if verbose:
         print(LIB)
     return LIB

@@ -27,6 +27,12 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
+}  // namespace
+
+int ftlm_b200::set_error(int code, const char* msg) { return fail(code, msg); }
+
+namespace {
+
 #define CU_TRY(expr)                                                                                     \
   do {                                                                                                   \
     cudaError_t e_ = (expr);                                                                             \
@@ -176,7 +182,7 @@ struct ftlm_sector {
   }
   int apply(const double2* x, double2* y, cudaStream_t st) {
     const int path = effective_path();
-    if (path == 2 && !hv_fast_path_ok(dev, plan.max_up_deg) && hv_rows_smem_bytes(dev) > 220 * 1024)
+    if (path == 2 && hv_rows_smem_bytes(dev) > 227 * 1024)
       return fail(FTLM_ERR_UNSUPPORTED, "row pass does not fit in shared memory for this sector");
     CU_TRY(hv_launch(dev, x, y, path, st));
     return FTLM_OK;
@@ -372,12 +378,31 @@ int ftlm_gpu_sector_index_of(const ftlm_sector* s, uint64_t up, uint64_t dn, lon
   return FTLM_OK;
 }
 
+int ftlm_gpu_sector_state(const ftlm_sector* s, long long index, uint64_t* up, uint64_t* dn) {
+  if (!s || !up || !dn) return fail(FTLM_ERR_INVALID, "null argument");
+  if (index < 0 || index >= s->plan.dim) return fail(FTLM_ERR_INVALID, "FockBasis index out of range");
+  *up = s->plan.up.masks[static_cast<size_t>(index / s->plan.dn.D)];
+  *dn = s->plan.dn.masks[static_cast<size_t>(index % s->plan.dn.D)];
+  return FTLM_OK;
+}
+
 int ftlm_gpu_sector_stats(const ftlm_sector* s, double* mean_up, double* mean_dn, long long* du, long long* dd) {
   if (!s) return fail(FTLM_ERR_INVALID, "null sector");
   if (mean_up) *mean_up = s->plan.mean_up_sources;
   if (mean_dn) *mean_dn = s->plan.mean_dn_sources;
   if (du) *du = s->plan.up.D;
   if (dd) *dd = s->plan.dn.D;
+  return FTLM_OK;
+}
+
+int ftlm_gpu_sector_down_table(const ftlm_sector* s, long long* n_groups, long long* n_entries, long long* gptr,
+                               uint32_t* entries, int* pad_hop) {
+  if (!s || !n_groups || !n_entries) return fail(FTLM_ERR_INVALID, "null argument");
+  *n_groups = static_cast<long long>(s->plan.dn_gptr.size()) - 1;
+  *n_entries = static_cast<long long>(s->plan.dn_ent.size());
+  if (gptr) std::copy(s->plan.dn_gptr.begin(), s->plan.dn_gptr.end(), gptr);
+  if (entries) std::copy(s->plan.dn_ent.begin(), s->plan.dn_ent.end(), entries);
+  if (pad_hop) *pad_hop = s->plan.dn_pad_hop;
   return FTLM_OK;
 }
 
@@ -484,6 +509,57 @@ int ftlm_gpu_lanczos_op(long long dim, ftlm_apply_fn fn, void* ctx, int max_step
   if (beta) std::copy(b.begin(), b.end(), beta);
   if (n_beta) *n_beta = static_cast<int>(b.size());
   if (used) *used = static_cast<int>(a.size());
+  return FTLM_OK;
+}
+
+int ftlm_gpu_lanczos_host_op(long long dim, ftlm_host_apply_fn fn, void* ctx, int max_steps, unsigned seed,
+                             int start_mode, double* alpha, double* beta, int* n_beta, int* used) {
+  if (!fn) return fail(FTLM_ERR_INVALID, "null operator");
+  LanczosWs ws;
+  std::vector<double> a, b, hx, hy;
+  try {
+    hx.resize(static_cast<size_t>(std::max(0LL, dim)) * 2);
+    hy.resize(static_cast<size_t>(std::max(0LL, dim)) * 2);
+  } catch (const std::bad_alloc&) {
+    return fail(FTLM_ERR_NOMEM, "host staging buffers");
+  }
+  const int rc = run_lanczos(
+      dim,
+      [&](const double2* x, double2* y, cudaStream_t st) {
+        CU_TRY(cudaMemcpyAsync(hx.data(), x, dim * sizeof(double2), cudaMemcpyDeviceToHost, st));
+        CU_TRY(cudaStreamSynchronize(st));
+        fn(hx.data(), hy.data(), ctx);
+        CU_TRY(cudaMemcpyAsync(y, hy.data(), dim * sizeof(double2), cudaMemcpyHostToDevice, st));
+        CU_TRY(cudaStreamSynchronize(st));
+        return FTLM_OK;
+      },
+      ws, max_steps, seed, start_mode, nullptr, &a, &b);
+  if (rc) return rc;
+  if (alpha) std::copy(a.begin(), a.end(), alpha);
+  if (beta) std::copy(b.begin(), b.end(), beta);
+  if (n_beta) *n_beta = static_cast<int>(b.size());
+  if (used) *used = static_cast<int>(a.size());
+  return FTLM_OK;
+}
+
+int ftlm_gpu_ftlm_combine(const double* logq, const double* energy_r, const int* used, int R, int n_bt, double log_dim,
+                          double* lnz, double* energy) {
+  if (R <= 0 || n_bt < 0 || !logq || !energy_r || !used || !lnz || !energy) return fail(FTLM_ERR_INVALID, "bad arguments");
+  if (n_bt == 0) return FTLM_OK;
+  const size_t qb = static_cast<size_t>(R) * n_bt * sizeof(double);
+  DevBuf dq, de, dn, dz, den;
+  CU_TRY(dq.alloc(qb));
+  CU_TRY(de.alloc(qb));
+  CU_TRY(dn.alloc(R * sizeof(int)));
+  CU_TRY(dz.alloc(n_bt * sizeof(double)));
+  CU_TRY(den.alloc(n_bt * sizeof(double)));
+  CU_TRY(cudaMemcpy(dq.p, logq, qb, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(de.p, energy_r, qb, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(dn.p, used, R * sizeof(int), cudaMemcpyHostToDevice));
+  CU_TRY(quad_sector(dq.as<double>(), de.as<double>(), dn.as<int>(), R, n_bt, log_dim, dz.as<double>(),
+                     den.as<double>(), nullptr));
+  CU_TRY(cudaMemcpy(lnz, dz.p, n_bt * sizeof(double), cudaMemcpyDeviceToHost));
+  CU_TRY(cudaMemcpy(energy, den.p, n_bt * sizeof(double), cudaMemcpyDeviceToHost));
   return FTLM_OK;
 }
 

@@ -96,13 +96,16 @@ __global__ void __launch_bounds__(kRowThreads, 1) hv_rows_kernel(DevSector S, co
       }
       xs[c] = v;
     }
-    for (int h = tid; h <= S.n_dn_hops; h += kRowThreads) {
+    // Per-row down-hop coefficients (c_h times the up-string JW factor), 8 copies so that the
+    // 8 lanes of a quarter-warp (lane % 8 = copy) never share a bank group.
+    for (int i = tid; i < (S.n_dn_hops + 1) * 8; i += kRowThreads) {
+      const int h = i >> 3;
       double2 cf = S.dn_coef[h];
       if (__popc(u & S.dn_nmask[h]) & 1) {
         cf.x = -cf.x;
         cf.y = -cf.y;
       }
-      coef[h] = cf;
+      coef[i] = cf;
     }
     if (saw_tiny) atomicOr(S.flags, 1);
     __syncthreads();
@@ -116,7 +119,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) hv_rows_kernel(DevSector S, co
 #pragma unroll 4
       for (int64_t p = S.dn_gptr[g] + (c & 31); p < e_end; p += 32) {
         const uint32_t ent = __ldg(S.dn_ent + p);
-        cmac(acc, coef[(ent >> 1) & 511u], xs[ent >> 10], ent & 1u);
+        cmac(acc, coef[((ent >> 1) & 511u) * 8 + (c & 7)], xs[ent >> 10], ent & 1u);
       }
       yrow[c] = acc;
     }
@@ -185,11 +188,11 @@ int g_num_sms = 0;
 }  // namespace
 
 size_t hv_rows_smem_bytes(const DevSector& S) {
-  return static_cast<size_t>(S.Dd) * sizeof(double2) + static_cast<size_t>(S.n_dn_hops + 1) * sizeof(double2);
+  return static_cast<size_t>(S.Dd) * sizeof(double2) + static_cast<size_t>(S.n_dn_hops + 1) * 8 * sizeof(double2);
 }
 
 bool hv_fast_path_ok(const DevSector& S, int max_up_deg) {
-  return hv_rows_smem_bytes(S) <= 220 * 1024 && max_up_deg <= kMaxUpDeg && S.dim >= (1 << 16);
+  return hv_rows_smem_bytes(S) <= 227 * 1024 && max_up_deg <= kMaxUpDeg && S.dim >= (1 << 16) && S.Dd >= 64;
 }
 
 void init_sm_count() {

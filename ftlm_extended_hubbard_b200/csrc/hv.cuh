@@ -49,4 +49,7 @@ cudaError_t gc_reduce_dev(const double* lnz_s, const double* e_s, const int* N_s
                           double* e_avg, cudaStream_t st);
 cudaError_t ritz_bisect(const double* alpha, const double* beta, int n, int k, double* ritz, cudaStream_t st);
 
+// Records an error message for ftlm_gpu_last_error() (capi.cu) and returns `code`.
+int set_error(int code, const char* msg);
+
 }  // namespace ftlm_b200

@@ -72,6 +72,85 @@ std::vector<MergedHop> merge_hops(const std::vector<HopIn>& hops, int spin) {
   return out;
 }
 
+// Orders the down-hop entries of one quarter-warp (8 lanes) into rounds so that in every round
+// the 8 lanes read 8 different shared-memory bank groups: an entry's group is src % 8 (16-byte
+// elements).  Edge-colouring of the bipartite multigraph lanes x groups with Delta colours
+// (Konig's theorem; alternating-path recolouring), Delta = max lane or group degree.  A lane idle
+// in a round reads an element of a group that round leaves free, with a zero coefficient.
+void schedule_quarter(const std::vector<uint32_t>* in, std::vector<uint32_t>* out, uint32_t pad_hop, int64_t Dd) {
+  struct Edge {
+    int lane, grp;
+    uint32_t ent;
+  };
+  std::vector<Edge> edges;
+  int degL[8] = {0}, degG[8] = {0};
+  for (int l = 0; l < 8; ++l)
+    for (uint32_t ent : in[l]) {
+      const int g = static_cast<int>((ent >> 10) & 7u);
+      edges.push_back(Edge{l, g, ent});
+      ++degL[l];
+      ++degG[g];
+    }
+  int D = 0;
+  for (int i = 0; i < 8; ++i) D = std::max(D, std::max(degL[i], degG[i]));
+  std::vector<int> atL(static_cast<size_t>(8 * std::max(D, 1)), -1), atG(static_cast<size_t>(8 * std::max(D, 1)), -1);
+  auto L = [&](int l, int c) -> int& { return atL[static_cast<size_t>(l * D + c)]; };
+  auto G = [&](int g, int c) -> int& { return atG[static_cast<size_t>(g * D + c)]; };
+  std::vector<int> col(edges.size(), -1);
+  for (size_t e = 0; e < edges.size(); ++e) {
+    const int l = edges[e].lane, g = edges[e].grp;
+    int a = 0, b = 0;
+    while (L(l, a) != -1) ++a;  // free at the lane
+    while (G(g, b) != -1) ++b;  // free at the group
+    if (G(g, a) != -1) {
+      // Swap colours a and b along the alternating path that leaves g on colour a.
+      std::vector<int> path;
+      bool at_group = true;
+      int v = g, c = a;
+      while (true) {
+        const int ed = at_group ? G(v, c) : L(v, c);
+        if (ed < 0) break;
+        path.push_back(ed);
+        v = at_group ? edges[static_cast<size_t>(ed)].lane : edges[static_cast<size_t>(ed)].grp;
+        at_group = !at_group;
+        c = (c == a) ? b : a;
+      }
+      for (int ed : path) {
+        const Edge& E = edges[static_cast<size_t>(ed)];
+        L(E.lane, col[static_cast<size_t>(ed)]) = -1;
+        G(E.grp, col[static_cast<size_t>(ed)]) = -1;
+      }
+      for (int ed : path) {
+        const Edge& E = edges[static_cast<size_t>(ed)];
+        const int nc = (col[static_cast<size_t>(ed)] == a) ? b : a;
+        col[static_cast<size_t>(ed)] = nc;
+        L(E.lane, nc) = ed;
+        G(E.grp, nc) = ed;
+      }
+    }
+    col[e] = a;
+    L(l, a) = static_cast<int>(e);
+    G(g, a) = static_cast<int>(e);
+  }
+  for (int l = 0; l < 8; ++l) out[l].assign(static_cast<size_t>(D), 0u);
+  for (int c = 0; c < D; ++c) {
+    int free_groups[8], nf = 0;
+    for (int g = 0; g < 8; ++g)
+      if (G(g, c) < 0) free_groups[nf++] = g;
+    int fi = 0;
+    for (int l = 0; l < 8; ++l) {
+      const int ed = L(l, c);
+      if (ed >= 0) {
+        out[l][static_cast<size_t>(c)] = edges[static_cast<size_t>(ed)].ent;
+      } else {
+        const int g = fi < nf ? free_groups[fi++] : 0;
+        const uint32_t src = static_cast<uint32_t>(g < Dd ? g : 0);
+        out[l][static_cast<size_t>(c)] = (src << 10) | pad_hop;
+      }
+    }
+  }
+}
+
 }  // namespace
 
 uint64_t binom(int n, int k) {
@@ -274,9 +353,10 @@ std::string build_plan(int n_sites, int n_up, int n_dn, double U, double V, cons
   const int64_t ngroups = (P.dn.D + 31) / 32;
   P.dn_gptr.assign(static_cast<size_t>(ngroups) + 1, 0);
   std::vector<std::vector<uint32_t>> lane(32);
+  std::vector<std::vector<uint32_t>> sched(32);
   int64_t total_src = 0;
+  const uint32_t pad_hop = static_cast<uint32_t>(P.dn_pad_hop) << 1;
   for (int64_t g = 0; g < ngroups; ++g) {
-    size_t K = 0;
     for (int l = 0; l < 32; ++l) {
       lane[l].clear();
       const int64_t r = g * 32 + l;
@@ -293,15 +373,22 @@ std::string build_plan(int n_sites, int n_up, int n_dn, double U, double V, cons
       }
       total_src += static_cast<int64_t>(lane[l].size());
       P.max_dn_deg = std::max(P.max_dn_deg, static_cast<int>(lane[l].size()));
-      K = std::max(K, lane[l].size());
+    }
+    // Per quarter-warp (8 lanes), order the entries so that in every round the 8 lanes read
+    // 8 different shared-memory bank groups (a 16-byte element src sits in group src % 8).
+    size_t K = 0;
+    for (int qw = 0; qw < 4; ++qw) {
+      schedule_quarter(&lane[8 * qw], &sched[8 * qw], pad_hop, P.dn.D);
+      K = std::max(K, sched[8 * qw].size());
+    }
+    for (int l = 0; l < 32; ++l) {
+      // Rounds a quarter does not need: every lane reads its own element (distinct groups).
+      const int64_t r = g * 32 + l;
+      const uint32_t self = static_cast<uint32_t>(r < P.dn.D ? r : std::min<int64_t>(l & 7, P.dn.D - 1));
+      while (sched[l].size() < K) sched[l].push_back((self << 10) | pad_hop);
     }
     for (size_t k = 0; k < K; ++k)
-      for (int l = 0; l < 32; ++l) {
-        const int64_t r = g * 32 + l;
-        const uint32_t self = static_cast<uint32_t>(r < P.dn.D ? r : 0);
-        P.dn_ent.push_back(k < lane[l].size() ? lane[l][k]
-                                              : ((self << 10) | (static_cast<uint32_t>(P.dn_pad_hop) << 1)));
-      }
+      for (int l = 0; l < 32; ++l) P.dn_ent.push_back(sched[l][k]);
     P.dn_gptr[static_cast<size_t>(g) + 1] = static_cast<int64_t>(P.dn_ent.size());
   }
   P.mean_dn_sources = P.dn.D ? static_cast<double>(total_src) / static_cast<double>(P.dn.D) : 0.0;

@@ -83,9 +83,16 @@ int ftlm_gpu_sector_destroy(ftlm_sector* s);
 int ftlm_gpu_sector_dim(const ftlm_sector* s, long long* dim);
 int ftlm_gpu_sector_masks(const ftlm_sector* s, uint64_t* up_host, uint64_t* dn_host);
 int ftlm_gpu_sector_index_of(const ftlm_sector* s, uint64_t up, uint64_t dn, long long* index);
+/* (up, down) strings of one state (FockBasis::up_mask/down_mask, include/ftlm/fock_basis.hpp:20-21). */
+int ftlm_gpu_sector_state(const ftlm_sector* s, long long index, uint64_t* up, uint64_t* dn);
 /* Mean number of distinct up-hop source rows per up string (the row-gather traffic model). */
 int ftlm_gpu_sector_stats(const ftlm_sector* s, double* mean_up_sources, double* mean_dn_sources, long long* du,
                           long long* dd);
+/* Host copy of the down-hop gather table (for inspection/tests): n_groups+1 group offsets and the
+ * entries (src_rank<<10 | hop_id<<1 | sign), 32 lanes interleaved per group.  Pass NULL buffers to
+ * query the sizes. */
+int ftlm_gpu_sector_down_table(const ftlm_sector* s, long long* n_groups, long long* n_entries, long long* gptr,
+                               uint32_t* entries, int* pad_hop);
 /* Diagonal entry H[i,i] (host computation from the sector tables). */
 int ftlm_gpu_sector_diag(const ftlm_sector* s, long long index, double* value);
 
@@ -114,6 +121,13 @@ typedef void (*ftlm_apply_fn)(const double* x_dev, double* y_dev, void* ctx);
 int ftlm_gpu_lanczos_op(long long dim, ftlm_apply_fn apply, void* ctx, int max_steps, unsigned seed, int start_mode,
                         double* alpha, double* beta, int* n_beta, int* used);
 
+/* Lanczos with a caller operator on HOST buffers, the std::function apply_h of lanczos_tridiagonal
+ * (include/ftlm/lanczos.hpp:55-59): vectors stay on the device; each step copies q to a host
+ * buffer, calls apply(x_host, y_host, ctx) and copies y back. */
+typedef void (*ftlm_host_apply_fn)(const double* x_host, double* y_host, void* ctx);
+int ftlm_gpu_lanczos_host_op(long long dim, ftlm_host_apply_fn apply, void* ctx, int max_steps, unsigned seed,
+                             int start_mode, double* alpha, double* beta, int* n_beta, int* used);
+
 /* Ritz values and first-row weights of n_chains tridiagonals (alpha/beta: [n_chains][ld]),
  * by the reference's classical Jacobi with max_rot rotations (<=0: max(3000,120n)) and tol.
  * lam/w0 outputs [n_chains][ld]; n[c] = size of chain c.  Host buffers. */
@@ -129,6 +143,11 @@ int ftlm_gpu_ritz_values(const double* alpha, const double* beta, int n, int k, 
  * (seed_r = seed + r*100003, src/ftlm_thermo.cpp:234), plus the FTLM energy <H>_s. */
 int ftlm_gpu_ftlm_sector(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed, int start_mode,
                          double* lnz, double* energy);
+
+/* Sector ln Z from R chain quadratures (src/ftlm_thermo.cpp:246-256): lnz[b] = log_dim +
+ * log mean_{r: used[r] > 0} e^{logq[r][b]}; energy = e^{logq}-weighted chain energies.  Host arrays. */
+int ftlm_gpu_ftlm_combine(const double* logq, const double* energy_r, const int* used, int R, int n_bt, double log_dim,
+                          double* lnz, double* energy);
 
 /* Grand-canonical combination over sectors (host arrays): lnz_s/e_s [n_sec][n_bt], N_s [n_sec];
  * outputs [n_bt][n_mu]: ln Z_GC, <n> per site, <E>. */

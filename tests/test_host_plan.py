@@ -133,3 +133,40 @@ def test_device_calls_fail_cleanly_without_gpu():
     with pytest.raises(F.FtlmError) as e:
         F.Sector(F.HubbardParams(2, 2, 1.0), 1, 1)
     assert e.value.code in (_lib.FTLM_ERR_CUDA, _lib.FTLM_ERR_NOMEM)
+
+
+@pytest.mark.parametrize("c", [(4, 4, 8, 8), (4, 4, 6, 5), (4, 3, 6, 6), (3, 3, 4, 5), (4, 4, 3, 1)])
+def test_down_table_schedule_is_bank_conflict_free(c):
+    """Every round of every quarter-warp reads 8 distinct bank groups (src % 8), and each lane keeps
+    exactly its valid down hops: the sources of its entries are the down strings one hop away."""
+    Lx, Ly, nu, nd = c
+    hops, pairs = F.build_hubbard_geometry(F.HubbardParams(Lx, Ly, 1.0, -0.25, 8.0, 1.0, 0.1, 0.0))
+    h = C.c_void_p()
+    _lib.call("ftlm_gpu_sector_create_host", Lx * Ly, nu, nd, 8.0, 1.0, F.api._c_hops(hops), len(hops),
+              F.api._c_pairs(pairs), len(pairs), C.byref(h))
+    ng, ne, pad = C.c_longlong(), C.c_longlong(), C.c_int()
+    _lib.call("ftlm_gpu_sector_down_table", h, C.byref(ng), C.byref(ne), None, None, C.byref(pad))
+    gptr = np.zeros(ng.value + 1, np.int64)
+    ent = np.zeros(ne.value, np.uint32)
+    _lib.call("ftlm_gpu_sector_down_table", h, C.byref(ng), C.byref(ne), gptr.ctypes.data_as(C.c_void_p),
+              ent.ctypes.data_as(C.c_void_p), C.byref(pad))
+    b = F.FockBasis(Lx * Ly, nd, 0)
+    dn, _ = b.masks()
+    Dd = dn.size
+    moves = {(x.from_, x.to) for x in hops if x.spin == 1}
+    for g in range(ng.value):
+        blk = ent[gptr[g]:gptr[g + 1]].reshape(-1, 32)
+        src = blk >> 10
+        hop = (blk >> 1) & 511
+        for qw in range(4):
+            for row in src[:, 8 * qw: 8 * qw + 8] % 8:
+                assert len(set(row.tolist())) == 8
+        for l in range(32):
+            r = 32 * g + l
+            if r >= Dd:
+                continue
+            d2 = int(dn[r])
+            expect = sorted(b.index_of(d2 ^ (1 << f) ^ (1 << t), 0) for f, t in moves
+                            if (d2 >> t) & 1 and not (d2 >> f) & 1)
+            assert sorted(src[:, l][hop[:, l] != pad.value].tolist()) == expect
+    _lib.lib().ftlm_gpu_sector_destroy(h)
