@@ -79,6 +79,7 @@ SIGNATURES = {
     "ftlm_gpu_tridiag_eig": [_vp, _vp, _vp, _i, _i, _i, _d, _vp, _vp],
     "ftlm_gpu_tridiag_quadrature": [_vp, _vp, _vp, _i, _i, _vp, _i, _vp, _vp],
     "ftlm_gpu_ritz_values": [_vp, _vp, _i, _i, _vp],
+    "ftlm_gpu_tridiag_quadrature_noalloc": [_vp, _vp, _vp, _i, _i, _vp, _i, _vp, _vp, _vp],
     "ftlm_gpu_ftlm_sector": [_vp, _vp, _i, _i, _i, C.c_uint, _i, _vp, _vp],
     "ftlm_gpu_gc_reduce": [_vp, _vp, _vp, _i, _vp, _i, _vp, _i, _i, _vp, _vp, _vp],
     "ftlm_gpu_gc_sweep": [C.POINTER(FtlmParams), _i, _i, C.c_uint, _i, _vp, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp],

@@ -136,6 +136,18 @@ int ftlm_gpu_tridiag_eig(const double* alpha, const double* beta, const int* n, 
 /* log sum_k w_k exp(-bT lam_k) per chain and temperature: out [n_chains][n_bt]. */
 int ftlm_gpu_tridiag_quadrature(const double* alpha, const double* beta, const int* n, int n_chains, int ld,
                                 const double* bts, int n_bt, double* logq, double* energy);
+/* ftlm_gpu_tridiag_quadrature on caller-owned DEVICE buffers that allocates nothing (no counterpart in
+ * the reference).  For callers that must not call cudaMalloc/cudaFree here: device memory owned by
+ * another allocator (e.g. a framework pool that has reserved most of HBM) or latency-critical loops
+ * where allocation would implicitly synchronise the device.  Intermediate Ritz pairs live in a
+ * library-owned 1 MiB __device__ array on every GPU that loads the library: n_chains*ld <= 65536,
+ * larger requests fail with FTLM_ERR_UNSUPPORTED.  Calls that overlap on the GPU race on that array
+ * (serialise them on one stream).  The first call on each device looks the array up with
+ * cudaGetSymbolAddress; make it before any stream capture on that device.  Work is enqueued on
+ * `stream`; the call does not synchronise. */
+int ftlm_gpu_tridiag_quadrature_noalloc(const double* alpha_dev, const double* beta_dev, const int* n_dev, int n_chains,
+                                        int ld, const double* bts_dev, int n_bt, double* logq_dev, double* energy_dev,
+                                        void* stream);
 /* Exact Ritz values (Sturm bisection, ascending) of one tridiagonal: lowest k into ritz[k]. */
 int ftlm_gpu_ritz_values(const double* alpha, const double* beta, int n, int k, double* ritz);
 
