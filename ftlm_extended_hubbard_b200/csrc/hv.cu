@@ -8,7 +8,7 @@
 //   hv_rows     pass 1 of the fast path: persistent CTAs, one output row at a time; the input
 //               row is staged in shared memory (down hops gather inside it); writes
 //               y = diag o x + down part.  Requires a down row (+ coefficient table) to fit in SMEM.
-//   hv_cols     pass 2: CTA = (output row, 256-column chunk), chunk-major launch order so that
+//   hv_cols     pass 2: CTA = (output row, 256-column chunk, two columns per thread), chunk-major so that
 //               the 256-column slab of x stays resident in L2 while all rows read it; adds the
 //               up part: y[r, c] += sum_j coef_j * s_j(c) * x[src_j, c].
 // Reference: src/hubbard_hamiltonian.cpp:51-108 (apply_extended_hubbard).
@@ -127,40 +127,69 @@ __global__ void __launch_bounds__(kRowThreads, 1) hv_rows_kernel(DevSector S, co
   }
 }
 
-constexpr int kColThreads = 256;
+constexpr int kColThreads = 128;           // two columns per thread: chunk = 256 columns
+constexpr int kColChunk = 2 * kColThreads;
 constexpr int kMaxUpDeg = 128;
+
+// acc += (-1)^neg c v, the sign applied to c's sign bits.
+__device__ __forceinline__ void cmac_xor(double2& acc, double2 c, double2 v, uint32_t neg) {
+  const int flip = static_cast<int>(neg << 31);
+  c.x = __hiloint2double(__double2hiint(c.x) ^ flip, __double2loint(c.x));
+  c.y = __hiloint2double(__double2hiint(c.y) ^ flip, __double2loint(c.y));
+  acc.x = fma(c.x, v.x, acc.x);
+  acc.x = fma(-c.y, v.y, acc.x);
+  acc.y = fma(c.x, v.y, acc.y);
+  acc.y = fma(c.y, v.x, acc.y);
+}
 
 template <bool kFilter>
 __device__ __forceinline__ void cols_body(const DevSector& S, const double2* __restrict__ x, double2* __restrict__ y,
-                                          int64_t r, int64_t c, int deg, const int* s_src, const double2* s_coef,
+                                          int64_t r, int64_t c0, int deg, const int64_t* s_off, const double2* s_coef,
                                           const uint32_t* s_lh) {
-  const uint32_t q = prefix_parity_shifted(S.dmask[c]);
-  double2 acc = y[r * S.Dd + c];
-  const double2* xc = x + c;
+  const int64_t c1 = c0 + kColThreads;
+  const bool has1 = c1 < S.Dd;
+  const int64_t c1s = has1 ? c1 : c0;  // in-bounds column for the second lane slot
+  const uint32_t q0 = prefix_parity_shifted(S.dmask[c0]);
+  const uint32_t q1 = prefix_parity_shifted(S.dmask[c1s]);
+  double2* y0 = y + r * S.Dd + c0;
+  double2 acc0 = *y0;
+  double2 acc1 = has1 ? y[r * S.Dd + c1] : make_double2(0.0, 0.0);
+  const double2* x0 = x + c0;
+  const double2* x1 = x + c1s;
   int j = 0;
-  for (; j + 8 <= deg; j += 8) {
-    double2 v[8];
+  for (; j + 4 <= deg; j += 4) {
+    double2 v0[4], v1[4];
 #pragma unroll
-    for (int t = 0; t < 8; ++t) v[t] = xc[static_cast<int64_t>(s_src[j + t]) * S.Dd];
+    for (int t = 0; t < 4; ++t) {
+      const int64_t off = s_off[j + t];
+      v0[t] = x0[off];
+      v1[t] = x1[off];
+    }
 #pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      if (kFilter && tiny(v[t])) continue;
+    for (int t = 0; t < 4; ++t) {
       const uint32_t lh = s_lh[j + t];
-      cmac(acc, s_coef[j + t], v[t], ((q >> (lh & 255u)) ^ (q >> (lh >> 8))) & 1u);
+      const uint32_t lo = lh & 255u, hi = lh >> 8;
+      const double2 cf = s_coef[j + t];
+      if (!kFilter || !tiny(v0[t])) cmac_xor(acc0, cf, v0[t], ((q0 >> lo) ^ (q0 >> hi)) & 1u);
+      if (!kFilter || !tiny(v1[t])) cmac_xor(acc1, cf, v1[t], ((q1 >> lo) ^ (q1 >> hi)) & 1u);
     }
   }
   for (; j < deg; ++j) {
-    const double2 v = xc[static_cast<int64_t>(s_src[j]) * S.Dd];
-    if (kFilter && tiny(v)) continue;
+    const int64_t off = s_off[j];
+    const double2 v0 = x0[off], v1 = x1[off];
     const uint32_t lh = s_lh[j];
-    cmac(acc, s_coef[j], v, ((q >> (lh & 255u)) ^ (q >> (lh >> 8))) & 1u);
+    const uint32_t lo = lh & 255u, hi = lh >> 8;
+    const double2 cf = s_coef[j];
+    if (!kFilter || !tiny(v0)) cmac_xor(acc0, cf, v0, ((q0 >> lo) ^ (q0 >> hi)) & 1u);
+    if (!kFilter || !tiny(v1)) cmac_xor(acc1, cf, v1, ((q1 >> lo) ^ (q1 >> hi)) & 1u);
   }
-  y[r * S.Dd + c] = acc;
+  *y0 = acc0;
+  if (has1) y[r * S.Dd + c1] = acc1;
 }
 
 __global__ void __launch_bounds__(kColThreads) hv_cols_kernel(DevSector S, const double2* __restrict__ x,
                                                               double2* __restrict__ y) {
-  __shared__ int s_src[kMaxUpDeg];
+  __shared__ int64_t s_off[kMaxUpDeg];
   __shared__ double2 s_coef[kMaxUpDeg];
   __shared__ uint32_t s_lh[kMaxUpDeg];
   const int64_t b = blockIdx.x;
@@ -169,18 +198,18 @@ __global__ void __launch_bounds__(kColThreads) hv_cols_kernel(DevSector S, const
   const int j0 = S.up_ptr[r];
   const int deg = S.up_ptr[r + 1] - j0;
   for (int j = threadIdx.x; j < deg; j += kColThreads) {
-    s_src[j] = S.up_src[j0 + j];
+    s_off[j] = static_cast<int64_t>(S.up_src[j0 + j]) * S.Dd;
     s_coef[j] = S.up_coef[j0 + j];
     s_lh[j] = S.up_lohi[j0 + j];
   }
   const bool filt = (*S.flags) != 0;
   __syncthreads();
-  const int64_t c = chunk * kColThreads + threadIdx.x;
-  if (c >= S.Dd) return;
+  const int64_t c0 = chunk * kColChunk + threadIdx.x;
+  if (c0 >= S.Dd) return;
   if (filt)
-    cols_body<true>(S, x, y, r, c, deg, s_src, s_coef, s_lh);
+    cols_body<true>(S, x, y, r, c0, deg, s_off, s_coef, s_lh);
   else
-    cols_body<false>(S, x, y, r, c, deg, s_src, s_coef, s_lh);
+    cols_body<false>(S, x, y, r, c0, deg, s_off, s_coef, s_lh);
 }
 
 int g_num_sms = 0;
@@ -217,7 +246,7 @@ cudaError_t hv_launch_pass(const DevSector& S, const double2* x, double2* y, int
     hv_rows_kernel<<<grid_r, kRowThreads, sm, st>>>(S, x, y);
     return cudaGetLastError();
   }
-  const int64_t nchunks = (S.Dd + kColThreads - 1) / kColThreads;
+  const int64_t nchunks = (S.Dd + kColChunk - 1) / kColChunk;
   const int64_t grid_c = nchunks * S.Du;
   hv_cols_kernel<<<static_cast<unsigned>(grid_c), kColThreads, 0, st>>>(S, x, y);
   return cudaGetLastError();
