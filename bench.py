@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--sector", type=int, nargs=2, default=None, metavar=("NU", "ND"),
                     help="profile a smaller 4x4 sector instead (for ncu captures); not a bench line")
+    ap.add_argument("--workload", default="hv", choices=["hv", "batched"],
+                    help="hv: the H·v benchmark; batched: 32-chain complex64 Lanczos steps on one sector "
+                         "(profiling aid, prints chain-steps/s)")
     return ap.parse_args()
 
 
@@ -362,10 +365,29 @@ def run_ours(args):
     return 0
 
 
+def run_batched(args):
+    """32 complex64 chains of one 4x4 sector for `steps` Lanczos steps (one CUDA graph)."""
+    import torch
+    import ftlm_extended_hubbard_b200 as F
+    nu, nd = args.sector if args.sector else (NU, ND)
+    sec = F.Sector(F.HubbardParams(**PARAMS), nu, nd)
+    sec.batched_lanczos(32, max(1, args.warmup), 7)  # allocation + warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sec.batched_lanczos(32, args.steps, 7)
+    t = time.perf_counter() - t0
+    print(json.dumps({"workload": f"batched Lanczos, 4x4 sector ({nu},{nd}), dim {sec.dim()}, 32 chains",
+                      "steps": args.steps, "seconds": t, "ms_per_chain_step": 1000.0 * t / (32 * args.steps)}))
+    F.batched_release()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batched":
+        return run_batched(args)
     return run_ours(args)
 
 

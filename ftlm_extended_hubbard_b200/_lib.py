@@ -82,6 +82,10 @@ SIGNATURES = {
     "ftlm_gpu_tridiag_quadrature_noalloc": [_vp, _vp, _vp, _i, _i, _vp, _i, _vp, _vp, _vp],
     "ftlm_gpu_ftlm_sector": [_vp, _vp, _i, _i, _i, C.c_uint, _i, _vp, _vp],
     "ftlm_gpu_gc_reduce": [_vp, _vp, _vp, _i, _vp, _i, _vp, _i, _i, _vp, _vp, _vp],
+    "ftlm_gpu_batched_lanczos": [_vp, _i, _i, C.c_uint, _vp, _vp, _vp],
+    "ftlm_gpu_batched_ftlm_sector": [_vp, _vp, _i, _i, _i, C.c_uint, _vp, _vp],
+    "ftlm_gpu_batched_sweep": [C.POINTER(FtlmParams), _i, _i, C.c_uint, _vp, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp],
+    "ftlm_gpu_batched_release": [],
     "ftlm_gpu_gc_sweep": [C.POINTER(FtlmParams), _i, _i, C.c_uint, _i, _vp, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp],
 }
 _RESTYPES = {"ftlm_gpu_last_error": C.c_char_p, "ftlm_gpu_version_string": C.c_char_p}

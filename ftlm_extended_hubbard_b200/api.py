@@ -263,6 +263,25 @@ class Sector(_Handle):
         return lnz, en
 
 
+    def batched_lanczos(self, n_random: int, lanczos_steps: int, seed: int):
+        """32-chain complex64 Lanczos: alpha/beta [R][M] (beta zero-padded), used [R]."""
+        R, M = n_random, lanczos_steps
+        a = np.zeros((R, M))
+        b = np.zeros((R, M))
+        u = np.zeros(R, np.int32)
+        call("ftlm_gpu_batched_lanczos", self._h, R, M, C.c_uint(seed & 0xFFFFFFFF), a.ctypes.data_as(C.c_void_p),
+             b.ctypes.data_as(C.c_void_p), u.ctypes.data_as(C.c_void_p))
+        return a, b, u
+
+    def batched_ftlm(self, betas, n_random: int, lanczos_steps: int, seed: int):
+        bt = np.ascontiguousarray(np.atleast_1d(np.asarray(betas, dtype=np.float64)))
+        lnz = np.zeros(bt.size)
+        en = np.zeros(bt.size)
+        call("ftlm_gpu_batched_ftlm_sector", self._h, bt.ctypes.data_as(C.c_void_p), bt.size, n_random,
+             lanczos_steps, C.c_uint(seed & 0xFFFFFFFF), lnz.ctypes.data_as(C.c_void_p), en.ctypes.data_as(C.c_void_p))
+        return lnz, en
+
+
 @dataclass
 class LanczosExtrema:
     min_eval: float = 0.0
@@ -325,6 +344,11 @@ def lanczos_tridiagonal(dim_or_sector, apply_h=None, max_steps: int = 0, seed: i
     if int(dim_or_sector) <= 0 or max_steps <= 0:
         return np.zeros(0), np.zeros(0), 0
     return _op_lanczos(int(dim_or_sector), apply_h, max_steps, seed, start)
+
+
+def batched_release():
+    """Frees the batched path's block vectors (kept between calls otherwise)."""
+    call("ftlm_gpu_batched_release")
 
 
 def tridiag_eig(alpha: np.ndarray, beta: np.ndarray, n: np.ndarray, max_rot: int = 0, tol: float = 1e-14):
@@ -432,8 +456,11 @@ class SweepResult:
 
 
 def grand_canonical_sweep(p: HubbardParams, n_random: int, lanczos_steps: int, seed: int, temperatures, mus,
-                          start: str = "reference") -> SweepResult:
-    """Plain path: every (N_up, N_dn) sector, R chains each, then the (T, mu) grid."""
+                          start: str = "reference", method: str = "plain") -> SweepResult:
+    """Every (N_up, N_dn) sector, R chains each, then the (T, mu) grid.
+
+    method "plain": complex128, one chain at a time (start "reference" or "philox");
+    method "batched": complex64 block vectors of 32 chains, Philox starts (see ftlm_gpu.h)."""
     T = np.ascontiguousarray(np.atleast_1d(temperatures), dtype=np.float64)
     bts = np.ascontiguousarray(1.0 / T)
     mu = np.ascontiguousarray(np.atleast_1d(mus), dtype=np.float64)
@@ -444,9 +471,13 @@ def grand_canonical_sweep(p: HubbardParams, n_random: int, lanczos_steps: int, s
     g1 = np.zeros((bts.size, mu.size))
     g2 = np.zeros_like(g1)
     g3 = np.zeros_like(g1)
-    call("ftlm_gpu_gc_sweep", C.byref(p._c()), n_random, lanczos_steps, C.c_uint(seed & 0xFFFFFFFF),
-         START_MODES[start], bts.ctypes.data_as(C.c_void_p), bts.size, mu.ctypes.data_as(C.c_void_p), mu.size,
-         lz.ctypes.data_as(C.c_void_p), es.ctypes.data_as(C.c_void_p), g1.ctypes.data_as(C.c_void_p),
-         g2.ctypes.data_as(C.c_void_p), g3.ctypes.data_as(C.c_void_p))
+    outs = [x.ctypes.data_as(C.c_void_p) for x in (lz, es, g1, g2, g3)]
+    if method == "batched":
+        call("ftlm_gpu_batched_sweep", C.byref(p._c()), n_random, lanczos_steps, C.c_uint(seed & 0xFFFFFFFF),
+             bts.ctypes.data_as(C.c_void_p), bts.size, mu.ctypes.data_as(C.c_void_p), mu.size, *outs)
+    else:
+        call("ftlm_gpu_gc_sweep", C.byref(p._c()), n_random, lanczos_steps, C.c_uint(seed & 0xFFFFFFFF),
+             START_MODES[start], bts.ctypes.data_as(C.c_void_p), bts.size, mu.ctypes.data_as(C.c_void_p), mu.size,
+             *outs)
     N = np.array([nu + nd for nu in range(n + 1) for nd in range(n + 1)])
     return SweepResult(T, bts, mu, lz, es, g1, g2, g3, N)

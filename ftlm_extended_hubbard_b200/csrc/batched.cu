@@ -1,0 +1,463 @@
+// Batched FTLM (complex64 vectors, FP64 scalars): the 32 Lanczos chains of one sector advance
+// together.  Block vectors are V[state][chain] (32 complex64 = 256 bytes per basis state), one
+// warp per basis state and lane = chain, so every gather is one coalesced 256-byte segment and the
+// index / JW-sign work of a hop is shared by the 32 chains.  Same hop tables as the complex128
+// path (plan.hpp), same recurrence as src/lanczos.cpp:180-205, with these changes of form:
+//
+//   * vectors are kept unnormalised: W_k = beta_{k-1} q_k (W_0 = raw start, beta_{-1} = ||raw||),
+//     and the 1/beta_{k-1} factor is applied to the H·v result in the kernel epilogue
+//       Y = H q_k = (H W_k) / beta_{k-1}
+//       z = <q_k, Y> = <W_k, Y> / beta_{k-1},  alpha_k = Re z
+//       W_{k+1} = Y - (z / beta_{k-1}) W_k - (beta_{k-1} / beta_{k-2}) W_{k-1},  beta_k = ||W_{k+1}||
+//     so no normalisation pass exists;
+//   * alpha/beta stay on the device; a chain whose ||w||^2 < 1e-24 stops (reference breakdown
+//     rule) and its later scale factors are 0;
+//   * H·v in FP32 (FMA), dot products and norms accumulated in FP64 with Neumaier compensation,
+//     the vector update evaluated in FP64 and rounded to complex64;
+//   * every kernel is persistent with a fixed grid (kBtBlocks) and fixed per-block work order, so
+//     the FP64 reductions are bitwise repeatable.
+#include <cstdio>
+
+#include "batched.cuh"
+#include "device.cuh"
+
+namespace ftlm_b200 {
+
+namespace {
+
+constexpr int kBtThreads = 256;  // 8 warps = 8 basis states per work item
+constexpr int kBtWarps = kBtThreads / 32;
+constexpr int kMaxUpDegB = 128;
+
+struct Neu {  // Neumaier-compensated FP64 sum
+  double s = 0.0, c = 0.0;
+  __device__ __forceinline__ void add(double v) {
+    const double t = s + v;
+    c += (fabs(s) >= fabs(v)) ? ((s - t) + v) : ((v - t) + s);
+    s = t;
+  }
+  __device__ __forceinline__ double value() const { return s + c; }
+};
+
+// |v|^2 < 1e-28 in FP32 (squares below FLT_MIN flush towards zero, which is still below the bound).
+__device__ __forceinline__ bool tinyf(float2 v) { return fmaf(v.x, v.x, v.y * v.y) < 1e-28f; }
+
+__device__ __forceinline__ void cmacf(float2& acc, float cr, float ci, float2 v, uint32_t neg) {
+  if (neg) {
+    cr = -cr;
+    ci = -ci;
+  }
+  acc.x = fmaf(cr, v.x, acc.x);
+  acc.x = fmaf(-ci, v.y, acc.x);
+  acc.y = fmaf(cr, v.y, acc.y);
+  acc.y = fmaf(ci, v.x, acc.y);
+}
+
+// Block-wide per-lane sum of NV doubles over the 8 warps; result valid in warp 0.
+template <int NV>
+__device__ __forceinline__ void lane_block_sum(double (&v)[NV], double* sh /* NV*kBtThreads */) {
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) sh[i * kBtThreads + t] = v[i];
+  __syncthreads();
+  if (t < 32) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      double s = 0.0;
+      for (int w = 0; w < kBtWarps; ++w) s += sh[i * kBtThreads + w * 32 + t];
+      v[i] = s;
+    }
+  }
+  __syncthreads();
+}
+
+// Start vectors: chain r uses Philox4x32-10 with key seed + r*100003 and counter = state index,
+// the same stream as the complex128 path's FTLM_START_PHILOX, rounded to complex64.
+__device__ __forceinline__ uint4 philox(uint4 c, uint2 k) {
+  constexpr uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
+    const uint32_t hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    k.x += W0;
+    k.y += W1;
+  }
+  return c;
+}
+
+__global__ void __launch_bounds__(kBtThreads) bt_start_kernel(float2* __restrict__ W, int64_t dim, unsigned seed,
+                                                              double* __restrict__ partial, int* __restrict__ flag) {
+  __shared__ double sh[kBtThreads];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned key = seed + static_cast<unsigned>(lane) * 100003u;
+  Neu acc;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * kBtWarps + warp; i < dim; i += static_cast<int64_t>(gridDim.x) * kBtWarps) {
+    const uint4 r = philox(make_uint4(static_cast<uint32_t>(i), static_cast<uint32_t>(i >> 32), 0u, 0u),
+                           make_uint2(key, 0x7F4A7C15u));
+    const uint64_t a = (static_cast<uint64_t>(r.x) << 21) ^ (r.y >> 11);
+    const uint64_t b = (static_cast<uint64_t>(r.z) << 21) ^ (r.w >> 11);
+    const double u1 = (static_cast<double>(a & ((1ull << 53) - 1)) + 0.5) * 0x1.0p-53;
+    const double u2 = (static_cast<double>(b & ((1ull << 53) - 1)) + 0.5) * 0x1.0p-53;
+    const double rad = sqrt(-2.0 * log(u1));
+    double s, c;
+    sincospi(2.0 * u2, &s, &c);
+    const float2 z = make_float2(static_cast<float>(rad * c), static_cast<float>(rad * s));
+    if (tinyf(z) && (z.x != 0.f || z.y != 0.f)) *flag = 1;
+    W[i * 32 + lane] = z;
+    acc.add(static_cast<double>(z.x) * z.x + static_cast<double>(z.y) * z.y);
+  }
+  double v[1] = {acc.value()};
+  lane_block_sum<1>(v, sh);
+  if (threadIdx.x < 32) partial[blockIdx.x * 32 + lane] = v[0];
+}
+
+constexpr int kBtUnroll = 4;  // hop pairs per batch: 8 independent 256-byte gathers per warp
+
+__device__ __forceinline__ float2 filt(float2 v) { return tinyf(v) ? make_float2(0.f, 0.f) : v; }
+__device__ __forceinline__ float4 filt4(float4 v) {
+  const float2 a = filt(make_float2(v.x, v.y)), b = filt(make_float2(v.z, v.w));
+  return make_float4(a.x, a.y, b.x, b.y);
+}
+
+// acc (two chains) += (-1)^neg c v with the sign applied to c's sign bits.
+__device__ __forceinline__ void cmac4(float4& acc, float2 c, float4 v, uint32_t neg) {
+  const uint32_t f = neg << 31;
+  c.x = __uint_as_float(__float_as_uint(c.x) ^ f);
+  c.y = __uint_as_float(__float_as_uint(c.y) ^ f);
+  acc.x = fmaf(c.x, v.x, acc.x);
+  acc.x = fmaf(-c.y, v.y, acc.x);
+  acc.y = fmaf(c.x, v.y, acc.y);
+  acc.y = fmaf(c.y, v.x, acc.y);
+  acc.z = fmaf(c.x, v.z, acc.z);
+  acc.z = fmaf(-c.y, v.w, acc.z);
+  acc.w = fmaf(c.x, v.w, acc.w);
+  acc.w = fmaf(c.y, v.z, acc.w);
+}
+
+__device__ __forceinline__ float4 fold_halves(float4 a) {
+  a.x += __shfl_down_sync(0xffffffffu, a.x, 16);
+  a.y += __shfl_down_sync(0xffffffffu, a.y, 16);
+  a.z += __shfl_down_sync(0xffffffffu, a.z, 16);
+  a.w += __shfl_down_sync(0xffffffffu, a.w, 16);
+  return a;
+}
+
+// Thread layout of both H·v passes: one warp per basis state; half-warp hv = lane >> 4 takes every
+// other hop, and lane l = lane & 15 holds chains 2l and 2l+1 (one float4), so one warp instruction
+// gathers two hops (2 x 256 bytes) and the per-hop index work is shared by 32 chains.
+
+// The walks below keep (row, column) as 32-bit counters advanced by the warp stride, so no
+// division runs per basis state; vector offsets are counted in float4 units (< 2^32 up to a
+// 68 GB block vector).
+
+// Row pass: Y[r, c, :] = s_in * (diag * W + down hops).  Warp-persistent over basis states in
+// row-major order (all warps of the grid walk the same row together, so the row of W —
+// Dd * 256 bytes — is served from L2).  Each warp keeps the down-hop coefficients of its current
+// row with the up-string JW factor folded in; no block barriers.
+template <bool kFilter>
+__device__ __forceinline__ void bt_rows_body(const DevSector& S, const float4* __restrict__ Wrow,
+                                             float4* __restrict__ Yrow, float4 sc, const float2* s_row, uint32_t u,
+                                             int cuu, uint4 wp, int c, int lane) {
+  const int hv = lane >> 4;
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (hv == 0) {
+    float4 xv = Wrow[static_cast<uint32_t>(c) * 16u];
+    if (kFilter) xv = filt4(xv);
+    const float dg = static_cast<float>(diag_value(S, u, S.dmask[c], cuu, S.cnt_dd[c], wp));
+    acc = make_float4(dg * xv.x, dg * xv.y, dg * xv.z, dg * xv.w);
+  }
+  // padded to a multiple of 8 entries: each half-warp takes 4 of every 8, no tail
+  const int64_t p0 = S.dn_csr_ptr[c];
+  const uint32_t* ent = S.dn_csr_ent + p0 + hv;
+  const int K = static_cast<int>(S.dn_csr_ptr[c + 1] - p0);
+  for (int k0 = 0; k0 < K; k0 += 8) {
+    uint32_t e[4];
+    float4 v[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) e[t] = ent[k0 + 2 * t];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) v[t] = Wrow[(e[t] >> 9) << 4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) cmac4(acc, s_row[e[t] & 511u], kFilter ? filt4(v[t]) : v[t], 0u);
+  }
+  acc = fold_halves(acc);
+  if (hv == 0)
+    Yrow[static_cast<uint32_t>(c) * 16u] = make_float4(acc.x * sc.x, acc.y * sc.x, acc.z * sc.z, acc.w * sc.z);
+}
+
+__global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_rows_kernel(DevSector S, const float2* __restrict__ W,
+                                                                             float2* __restrict__ Y,
+                                                                             const double* __restrict__ st,
+                                                                             const int* __restrict__ flag) {
+  __shared__ float2 s_row[kBtWarps][512];  // [2*hop + down-string sign], up-string sign folded in
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int l = lane & 15;
+  const float4 sc = make_float4(static_cast<float>(st[kBtSin * 32 + 2 * l]), 0.f,
+                                static_cast<float>(st[kBtSin * 32 + 2 * l + 1]), 0.f);
+  const bool filter = *flag != 0;
+  const int Dd = static_cast<int>(S.Dd), Du = static_cast<int>(S.Du);
+  const int gw = blockIdx.x * kBtWarps + warp;
+  const int nw = gridDim.x * kBtWarps;
+  float2* tab = s_row[warp];
+  int r = gw / Dd, c = gw - (gw / Dd) * Dd;
+  int cur_row = -1;
+  uint32_t u = 0;
+  int cuu = 0;
+  uint4 wp = make_uint4(0, 0, 0, 0);
+  while (r < Du) {
+    if (r != cur_row) {
+      __syncwarp();
+      u = S.umask[r];
+      cuu = S.cnt_uu[r];
+      wp = S.wpl[r];
+      for (int i = lane; i < 2 * (S.n_dn_hops + 1); i += 32) {
+        const int h = i >> 1;
+        const float2 cf = S.dn_coef32[h];
+        const float sg = ((__popc(u & S.dn_nmask[h]) ^ i) & 1) ? -1.f : 1.f;
+        tab[i] = make_float2(sg * cf.x, sg * cf.y);
+      }
+      __syncwarp();
+      cur_row = r;
+    }
+    const float4* Wrow = reinterpret_cast<const float4*>(W) + static_cast<int64_t>(r) * Dd * 16 + l;
+    float4* Yrow = reinterpret_cast<float4*>(Y) + static_cast<int64_t>(r) * Dd * 16 + l;
+    if (filter)
+      bt_rows_body<true>(S, Wrow, Yrow, sc, tab, u, cuu, wp, c, lane);
+    else
+      bt_rows_body<false>(S, Wrow, Yrow, sc, tab, u, cuu, wp, c, lane);
+    c += nw;
+    while (c >= Dd) {
+      c -= Dd;
+      ++r;
+    }
+  }
+}
+
+// Column pass: Y[r, c, :] += s_in * sum_j coef_j s_j(c) W[src_j, c, :], then the fused dot
+// <W_k, Y> per chain.  Warp-persistent over basis states in column-major order (the grid walks
+// one column of W at a time: Du * 256 bytes in L2).  Each warp builds its state's signed
+// coefficient list (padded to a multiple of 8 with zero coefficients) in its own shared-memory
+// slot; block barriers only for the final dot sums.
+template <bool kFilter>
+__device__ __forceinline__ float4 bt_cols_sum(const float4* Wc, const uint32_t* s_off, const float2* s_cf, int deg8,
+                                              int hv) {
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int j0 = hv; j0 < deg8; j0 += 8) {
+    float4 v[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) v[t] = Wc[s_off[j0 + 2 * t]];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) cmac4(acc, s_cf[j0 + 2 * t], kFilter ? filt4(v[t]) : v[t], 0u);
+  }
+  return fold_halves(acc);
+}
+
+__global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_cols_kernel(DevSector S, const float2* __restrict__ W,
+                                                                             float2* __restrict__ Y,
+                                                                             const double* __restrict__ st,
+                                                                             double* __restrict__ partial,
+                                                                             const int* __restrict__ flag) {
+  __shared__ uint32_t s_off[kBtWarps][kMaxUpDegB];
+  __shared__ float2 s_cf[kBtWarps][kMaxUpDegB];
+  __shared__ double sh[4 * kBtThreads];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int hv = lane >> 4, l = lane & 15;
+  const float4 sc = make_float4(static_cast<float>(st[kBtSin * 32 + 2 * l]), 0.f,
+                                static_cast<float>(st[kBtSin * 32 + 2 * l + 1]), 0.f);
+  const bool filter = *flag != 0;
+  const int Dd = static_cast<int>(S.Dd), Du = static_cast<int>(S.Du);
+  const uint32_t row_stride = static_cast<uint32_t>(Dd) * 16u;  // float4 units per row
+  const float4* W4 = reinterpret_cast<const float4*>(W);
+  float4* Y4 = reinterpret_cast<float4*>(Y);
+  const int gw = blockIdx.x * kBtWarps + warp;
+  const int nw = gridDim.x * kBtWarps;
+  uint32_t* off = s_off[warp];
+  float2* cfs = s_cf[warp];
+  double d0r = 0.0, d0i = 0.0, d1r = 0.0, d1i = 0.0;  // chains 2l and 2l+1 (half-warp 0 only)
+  int c = gw / Du, r = gw - (gw / Du) * Du;  // column-major walk
+  while (c < Dd) {
+    const int j0 = S.up_ptr[r];
+    const int deg = S.up_ptr[r + 1] - j0;
+    const uint32_t q = prefix_parity_shifted(S.dmask[c]);
+    const int deg8 = (deg + 7) & ~7;
+    __syncwarp();
+    for (int j = lane; j < deg8; j += 32) {
+      if (j < deg) {
+        off[j] = static_cast<uint32_t>(S.up_src[j0 + j]) * row_stride;
+        const uint32_t lh = S.up_lohi[j0 + j];
+        const uint32_t f = (((q >> (lh & 255u)) ^ (q >> (lh >> 8))) & 1u) << 31;
+        const float2 cd = S.up_coef32[j0 + j];
+        cfs[j] = make_float2(__uint_as_float(__float_as_uint(cd.x) ^ f), __uint_as_float(__float_as_uint(cd.y) ^ f));
+      } else {  // padding: a valid address, zero coefficient
+        off[j] = static_cast<uint32_t>(r) * row_stride;
+        cfs[j] = make_float2(0.f, 0.f);
+      }
+    }
+    __syncwarp();
+    const float4* Wc = W4 + static_cast<uint32_t>(c) * 16u + l;
+    const float4 acc = filter ? bt_cols_sum<true>(Wc, off, cfs, deg8, hv) : bt_cols_sum<false>(Wc, off, cfs, deg8, hv);
+    if (hv == 0) {
+      const int64_t o = static_cast<int64_t>(r) * row_stride + static_cast<uint32_t>(c) * 16u + l;
+      float4 y = Y4[o];
+      y.x = fmaf(acc.x, sc.x, y.x);
+      y.y = fmaf(acc.y, sc.x, y.y);
+      y.z = fmaf(acc.z, sc.z, y.z);
+      y.w = fmaf(acc.w, sc.z, y.w);
+      Y4[o] = y;
+      const float4 w = W4[o];
+      // conj(w) * y per chain
+      const double wx = w.x, wy = w.y, wz = w.z, ww = w.w;
+      const double yx = y.x, yy = y.y, yz = y.z, yw = y.w;
+      d0r = fma(wx, yx, fma(wy, yy, d0r));
+      d0i = fma(wx, yy, fma(-wy, yx, d0i));
+      d1r = fma(wz, yz, fma(ww, yw, d1r));
+      d1i = fma(wz, yw, fma(-ww, yz, d1i));
+    }
+    r += nw;
+    while (r >= Du) {
+      r -= Du;
+      ++c;
+    }
+  }
+  // per-chain block sums: lane l of every warp holds chains 2l, 2l+1
+  const int t = threadIdx.x;
+  sh[0 * kBtThreads + t] = d0r;
+  sh[1 * kBtThreads + t] = d0i;
+  sh[2 * kBtThreads + t] = d1r;
+  sh[3 * kBtThreads + t] = d1i;
+  __syncthreads();
+  if (t < 32) {
+    const int ll = t & 15, which = t >> 4;  // thread t reduces chain 2*ll + which
+    double re = 0.0, im = 0.0;
+    for (int w = 0; w < kBtWarps; ++w) {
+      re += sh[(2 * which) * kBtThreads + w * 32 + ll];
+      im += sh[(2 * which + 1) * kBtThreads + w * 32 + ll];
+    }
+    const int chain = 2 * ll + which;
+    partial[(blockIdx.x * 32 + chain) * 2] = re;
+    partial[(blockIdx.x * 32 + chain) * 2 + 1] = im;
+  }
+}
+
+// W_{k+1} = Y - c1 W_k - c2 W_{k-1} (in Y's buffer), ||W_{k+1}||^2 partials per chain.
+__global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_update_kernel(float2* __restrict__ Y,
+                                                                               const float2* __restrict__ Wk,
+                                                                               const float2* __restrict__ Wkm1,
+                                                                               int64_t dim, const double* __restrict__ st,
+                                                                               int use_prev, double* __restrict__ partial,
+                                                                               int* __restrict__ flag) {
+  __shared__ double sh[kBtThreads];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const double c1r = st[kBtC1r * 32 + lane], c1i = st[kBtC1i * 32 + lane];
+  const double c2 = use_prev ? st[kBtC2 * 32 + lane] : 0.0;
+  Neu acc;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * kBtWarps;
+  for (int64_t i0 = static_cast<int64_t>(blockIdx.x) * kBtWarps + warp; i0 < dim; i0 += 4 * stride) {
+    float2 y[4], a[4], b[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int64_t i = i0 + t * stride;
+      const int64_t o = (i < dim ? i : i0) * 32 + lane;
+      y[t] = Y[o];
+      a[t] = Wk[o];
+      b[t] = use_prev ? Wkm1[o] : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int64_t i = i0 + t * stride;
+      if (i >= dim) continue;
+      double wr = static_cast<double>(y[t].x) - (c1r * a[t].x - c1i * a[t].y);
+      double wi = static_cast<double>(y[t].y) - (c1r * a[t].y + c1i * a[t].x);
+      wr -= c2 * b[t].x;
+      wi -= c2 * b[t].y;
+      const float2 w = make_float2(static_cast<float>(wr), static_cast<float>(wi));
+      if (tinyf(w) && (w.x != 0.f || w.y != 0.f)) *flag = 1;
+      Y[i * 32 + lane] = w;
+      acc.add(static_cast<double>(w.x) * w.x + static_cast<double>(w.y) * w.y);
+    }
+  }
+  double v[1] = {acc.value()};
+  lane_block_sum<1>(v, sh);
+  if (threadIdx.x < 32) partial[blockIdx.x * 32 + lane] = v[0];
+}
+
+// One warp: chain lane.  mode 0: start norms -> s_in = 1/||raw||, c2 = 0.
+// mode 1: dot partials -> z, alpha_k, c1 = z * s_in.  mode 2: norm partials -> beta_k, next
+// s_in = 1/beta_k, c2 = beta_k * s_in (old), breakdown bookkeeping.
+__global__ void bt_scalar_kernel(const double* __restrict__ partial, int nblocks, int mode, int k,
+                                 double* __restrict__ st, double* __restrict__ alpha, double* __restrict__ beta,
+                                 int* __restrict__ used) {
+  const int lane = threadIdx.x;
+  if (lane >= 32) return;
+  if (mode == 1) {
+    Neu sr, si;
+    for (int b = 0; b < nblocks; ++b) {
+      sr.add(partial[(b * 32 + lane) * 2]);
+      si.add(partial[(b * 32 + lane) * 2 + 1]);
+    }
+    const double s_in = st[kBtSin * 32 + lane];
+    const double zr = sr.value() * s_in, zi = si.value() * s_in;
+    st[kBtC1r * 32 + lane] = zr * s_in;
+    st[kBtC1i * 32 + lane] = zi * s_in;
+    if (st[kBtActive * 32 + lane] != 0.0) alpha[k * 32 + lane] = zr;
+    return;
+  }
+  Neu s;
+  for (int b = 0; b < nblocks; ++b) s.add(partial[b * 32 + lane]);
+  const double n2 = s.value();
+  if (mode == 0) {
+    const double n0 = sqrt(n2);
+    st[kBtSin * 32 + lane] = (n0 < 1e-18) ? 0.0 : 1.0 / n0;
+    st[kBtC2 * 32 + lane] = 0.0;
+    st[kBtActive * 32 + lane] = (n0 < 1e-18) ? 0.0 : 1.0;
+    used[lane] = 0;
+    return;
+  }
+  const bool active = st[kBtActive * 32 + lane] != 0.0;
+  const double s_in = st[kBtSin * 32 + lane];
+  if (!active) {
+    st[kBtSin * 32 + lane] = 0.0;
+    st[kBtC2 * 32 + lane] = 0.0;
+    return;
+  }
+  used[lane] = k + 1;
+  if (n2 < 1e-24) {  // breakdown (src/lanczos.cpp:187): alpha_k kept, no beta_k
+    st[kBtActive * 32 + lane] = 0.0;
+    st[kBtSin * 32 + lane] = 0.0;
+    st[kBtC2 * 32 + lane] = 0.0;
+    return;
+  }
+  const double b = sqrt(n2);
+  beta[k * 32 + lane] = b;
+  st[kBtC2 * 32 + lane] = b * s_in;
+  st[kBtSin * 32 + lane] = 1.0 / b;
+}
+
+}  // namespace
+
+cudaError_t bt_start(float2* W, int64_t dim, unsigned seed, double* st, double* partial, int* used, int* flags,
+                     cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(flags, 0, 2 * sizeof(int), s);
+  if (e != cudaSuccess) return e;
+  bt_start_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(W, dim, seed, partial, flags);
+  bt_scalar_kernel<<<1, 32, 0, s>>>(partial, kBtBlocks, 0, 0, st, nullptr, nullptr, used);
+  return cudaGetLastError();
+}
+
+cudaError_t bt_step(const DevSector& S, const float2* Wk, const float2* Wkm1, float2* Y, int k, double* st,
+                    double* partial, double* alpha, double* beta, int* used, int* flags, cudaStream_t s) {
+  // flags[k % 2]: written vector W_k has a tiny non-zero entry; flags[(k+1) % 2] is cleared for W_{k+1}.
+  int* fin = flags + (k & 1);
+  int* fout = flags + ((k + 1) & 1);
+  cudaError_t e = cudaMemsetAsync(fout, 0, sizeof(int), s);
+  if (e != cudaSuccess) return e;
+  bt_rows_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(S, Wk, Y, st, fin);
+  bt_cols_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(S, Wk, Y, st, partial, fin);
+  bt_scalar_kernel<<<1, 32, 0, s>>>(partial, kBtBlocks, 1, k, st, alpha, beta, used);
+  bt_update_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(Y, Wk, Wkm1, S.dim, st, k > 0, partial, fout);
+  bt_scalar_kernel<<<1, 32, 0, s>>>(partial, kBtBlocks, 2, k, st, alpha, beta, used);
+  return cudaGetLastError();
+}
+
+}  // namespace ftlm_b200

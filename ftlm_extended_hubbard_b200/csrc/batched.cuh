@@ -1,0 +1,30 @@
+// Batched complex64 FTLM kernels (batched.cu): 32 chains of one sector per block vector.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+
+namespace ftlm_b200 {
+
+constexpr int kBtBlocksPerSm = 5;
+constexpr int kBtBlocks = kBtBlocksPerSm * 148;  // fixed persistent grid: deterministic reductions
+constexpr int kBtChains = 32;   // chains per block vector (one warp lane each)
+// Per-chain scalar state, st[field * 32 + chain] (doubles).
+constexpr int kBtSin = 0;     // 1 / beta_{k-1}: scale of H W_k
+constexpr int kBtC1r = 1;     // z / beta_{k-1} (coefficient of W_k), real and imaginary parts
+constexpr int kBtC1i = 2;
+constexpr int kBtC2 = 3;      // beta_{k-1} / beta_{k-2} (coefficient of W_{k-1})
+constexpr int kBtActive = 4;  // 1 while the chain has not broken down
+constexpr int kBtFields = 8;
+constexpr int kBtPartialDoubles = kBtBlocks * kBtChains * 2;
+
+// W <- complex64 Philox start vectors (chain r: key seed + r*100003), norms -> scalar state.
+// flags: 2 ints (tiny-entry flags of the current and next vector, cleared here).
+cudaError_t bt_start(float2* W, int64_t dim, unsigned seed, double* st, double* partial, int* used, int* flags,
+                     cudaStream_t s);
+// One Lanczos step k for all chains: Y <- H q_k, z, W_{k+1} (into Y), beta_k; alpha/beta [M][32].
+cudaError_t bt_step(const DevSector& S, const float2* Wk, const float2* Wkm1, float2* Y, int k, double* st,
+                    double* partial, double* alpha, double* beta, int* used, int* flags, cudaStream_t s);
+
+}  // namespace ftlm_b200

@@ -7,12 +7,14 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <mutex>
 #include <new>
 #include <random>
 #include <string>
 #include <vector>
 
 #include "../../include/ftlm_gpu.h"
+#include "batched.cuh"
 #include "hv.cuh"
 #include "plan.hpp"
 
@@ -204,13 +206,27 @@ int upload_plan(ftlm_sector* s) {
   std::vector<uint4> w4(static_cast<size_t>(P.up.D));
   for (size_t i = 0; i < w4.size(); ++i) w4[i] = make_uint4(P.wpl[4 * i], P.wpl[4 * i + 1], P.wpl[4 * i + 2], P.wpl[4 * i + 3]);
   std::vector<double2> upc(P.up_src.size()), dnc(P.dn_coef.size() / 2);
-  for (size_t i = 0; i < upc.size(); ++i) upc[i] = make_double2(P.up_coef[2 * i], P.up_coef[2 * i + 1]);
-  for (size_t i = 0; i < dnc.size(); ++i) dnc[i] = make_double2(P.dn_coef[2 * i], P.dn_coef[2 * i + 1]);
+  std::vector<float2> upc32(upc.size()), dnc32(dnc.size());
+  for (size_t i = 0; i < upc.size(); ++i) {
+    upc[i] = make_double2(P.up_coef[2 * i], P.up_coef[2 * i + 1]);
+    upc32[i] = make_float2(static_cast<float>(upc[i].x), static_cast<float>(upc[i].y));
+  }
+  for (size_t i = 0; i < dnc.size(); ++i) {
+    dnc[i] = make_double2(P.dn_coef[2 * i], P.dn_coef[2 * i + 1]);
+    dnc32[i] = make_float2(static_cast<float>(dnc[i].x), static_cast<float>(dnc[i].y));
+  }
+  float2 *ucf32, *dcf32;
+  CU_TRY(upload(upc32, &ucf32, &s->owned));
+  CU_TRY(upload(dnc32, &dcf32, &s->owned));
   uint32_t *um, *dm, *ulh, *dent, *dnm;
   int32_t *cuu, *cdd, *uptr, *usrc;
   uint4* wp;
   double2 *ucf, *dcf;
   int64_t* gptr;
+  int64_t* cptr;
+  uint32_t* cent;
+  CU_TRY(upload(P.dn_csr_ptr, &cptr, &s->owned));
+  CU_TRY(upload(P.dn_csr_ent, &cent, &s->owned));
   CU_TRY(upload(P.up.masks, &um, &s->owned));
   CU_TRY(upload(P.dn.masks, &dm, &s->owned));
   CU_TRY(upload(P.cnt_uu, &cuu, &s->owned));
@@ -238,6 +254,10 @@ int upload_plan(ftlm_sector* s) {
   D.up_lohi = ulh;
   D.dn_gptr = gptr;
   D.dn_ent = dent;
+  D.dn_csr_ptr = cptr;
+  D.up_coef32 = ucf32;
+  D.dn_coef32 = dcf32;
+  D.dn_csr_ent = cent;
   D.dn_coef = dcf;
   D.dn_nmask = dnm;
   D.n_dn_hops = P.dn_pad_hop;
@@ -763,6 +783,188 @@ int ftlm_gpu_gc_sweep(const ftlm_params* p, int R, int M, unsigned seed, int sta
     }
   if (lnz_gc && n_avg && e_avg)
     return ftlm_gpu_gc_reduce(lnz_s, e_s, N.data(), nsec, bts, n_bt, mus, n_mu, n, lnz_gc, n_avg, e_avg);
+  return FTLM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Batched complex64 FTLM (batched.cu): 32 chains per block vector, the M Lanczos steps of a block
+// captured once into a CUDA graph and launched without host synchronisation.
+namespace {
+
+struct BtWs {
+  int64_t cap = 0;
+  int mcap = 0;
+  DevBuf buf[3], st, partial, alpha, beta, used, flags;
+  cudaError_t ensure(int64_t dim, int M) {
+    cudaError_t e = cudaSuccess;
+    if (dim > cap) {
+      for (auto& b : buf) b.alloc(0);  // release before growing
+      for (auto& b : buf)
+        if ((e = b.alloc(static_cast<size_t>(dim) * kBtChains * sizeof(float2))) != cudaSuccess) return e;
+      cap = dim;
+    }
+    if (!st.p) {
+      if ((e = st.alloc(kBtFields * kBtChains * sizeof(double))) != cudaSuccess) return e;
+      if ((e = partial.alloc(kBtPartialDoubles * sizeof(double))) != cudaSuccess) return e;
+      if ((e = used.alloc(kBtChains * sizeof(int))) != cudaSuccess) return e;
+      if ((e = flags.alloc(2 * sizeof(int))) != cudaSuccess) return e;
+    }
+    if (M > mcap) {
+      if ((e = alpha.alloc(static_cast<size_t>(M) * kBtChains * sizeof(double))) != cudaSuccess) return e;
+      if ((e = beta.alloc(static_cast<size_t>(M) * kBtChains * sizeof(double))) != cudaSuccess) return e;
+      mcap = M;
+    }
+    return e;
+  }
+  void release() {
+    for (auto& b : buf) b.alloc(0);
+    cap = 0;
+  }
+};
+
+BtWs g_bt;
+std::mutex g_bt_mu;
+
+// Runs ceil(R/32) blocks of 32 chains on sector s; A/B [R][M] (beta zero-padded), used [R].
+int bt_run_chains(ftlm_sector* s, int R, int M, unsigned seed, std::vector<double>* A, std::vector<double>* B,
+                  std::vector<int>* used) {
+  const int64_t dim = s->plan.dim;
+  A->assign(static_cast<size_t>(R) * M, 0.0);
+  B->assign(static_cast<size_t>(R) * M, 0.0);
+  used->assign(static_cast<size_t>(R), 0);
+  std::lock_guard<std::mutex> lock(g_bt_mu);
+  CU_TRY(g_bt.ensure(dim, M));
+  cudaStream_t st = s->stream;
+  float2* bufs[3] = {g_bt.buf[0].as<float2>(), g_bt.buf[1].as<float2>(), g_bt.buf[2].as<float2>()};
+  double* sd = g_bt.st.as<double>();
+  double* part = g_bt.partial.as<double>();
+  double* al = g_bt.alpha.as<double>();
+  double* be = g_bt.beta.as<double>();
+  int* us = g_bt.used.as<int>();
+  int* fl = g_bt.flags.as<int>();
+  std::vector<double> ha(static_cast<size_t>(M) * kBtChains), hb(static_cast<size_t>(M) * kBtChains);
+  std::vector<int> hu(kBtChains);
+  for (int blk = 0; blk * kBtChains < R; ++blk) {
+    const unsigned seed_b = seed + static_cast<unsigned>(blk * kBtChains) * 100003u;
+    CU_TRY(cudaMemsetAsync(al, 0, static_cast<size_t>(M) * kBtChains * sizeof(double), st));
+    CU_TRY(cudaMemsetAsync(be, 0, static_cast<size_t>(M) * kBtChains * sizeof(double), st));
+    CU_TRY(bt_start(bufs[0], dim, seed_b, sd, part, us, fl, st));
+    cudaGraph_t graph = nullptr;
+    CU_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    float2 *wk = bufs[0], *y = bufs[1], *wkm1 = bufs[2];
+    cudaError_t ce = cudaSuccess;
+    for (int k = 0; k < M && ce == cudaSuccess; ++k) {
+      ce = bt_step(s->dev, wk, wkm1, y, k, sd, part, al, be, us, fl, st);
+      float2* t = wkm1;
+      wkm1 = wk;
+      wk = y;
+      y = t;
+    }
+    const cudaError_t ee = cudaStreamEndCapture(st, &graph);
+    if (ce != cudaSuccess || ee != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      return fail(FTLM_ERR_CUDA, std::string("batched step capture: ") +
+                                     cudaGetErrorString(ce != cudaSuccess ? ce : ee));
+    }
+    cudaGraphExec_t exec = nullptr;
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return fail(FTLM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+    ce = cudaGraphLaunch(exec, st);
+    const cudaError_t se = cudaStreamSynchronize(st);
+    cudaGraphExecDestroy(exec);
+    if (ce != cudaSuccess || se != cudaSuccess)
+      return fail(FTLM_ERR_CUDA, std::string("batched steps: ") + cudaGetErrorString(ce != cudaSuccess ? ce : se));
+    CU_TRY(cudaMemcpy(ha.data(), al, ha.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    CU_TRY(cudaMemcpy(hb.data(), be, hb.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    CU_TRY(cudaMemcpy(hu.data(), us, hu.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    for (int r = 0; r < kBtChains; ++r) {
+      const int ch = blk * kBtChains + r;
+      if (ch >= R) break;
+      (*used)[static_cast<size_t>(ch)] = hu[static_cast<size_t>(r)];
+      for (int k = 0; k < M; ++k) {
+        (*A)[static_cast<size_t>(ch) * M + k] = ha[static_cast<size_t>(k) * kBtChains + r];
+        (*B)[static_cast<size_t>(ch) * M + k] = hb[static_cast<size_t>(k) * kBtChains + r];
+      }
+    }
+  }
+  return FTLM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ftlm_gpu_batched_lanczos(ftlm_sector* s, int R, int M, unsigned seed, double* alpha, double* beta, int* used) {
+  int rc = need_device(s);
+  if (rc) return rc;
+  if (s->plan.max_up_deg > 120)
+    return fail(FTLM_ERR_UNSUPPORTED, "batched path: more than 120 up-hop sources per string");
+  if (R <= 0 || M <= 0 || !alpha || !beta || !used) return fail(FTLM_ERR_INVALID, "bad arguments");
+  std::vector<double> A, B;
+  std::vector<int> u;
+  rc = bt_run_chains(s, R, M, seed, &A, &B, &u);
+  if (rc) return rc;
+  std::copy(A.begin(), A.end(), alpha);
+  std::copy(B.begin(), B.end(), beta);
+  std::copy(u.begin(), u.end(), used);
+  return FTLM_OK;
+}
+
+int ftlm_gpu_batched_ftlm_sector(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed, double* lnz,
+                                 double* energy) {
+  int rc = need_device(s);
+  if (rc) return rc;
+  if (n_bt < 0 || (n_bt > 0 && (!bts || !lnz || !energy))) return fail(FTLM_ERR_INVALID, "bad arguments");
+  R = std::max(1, R);
+  M = std::max(1, M);
+  if (M > 160) return fail(FTLM_ERR_UNSUPPORTED, "more than 160 Lanczos steps for the on-chip Jacobi");
+  const int64_t dim = s->plan.dim;
+  // Sectors whose Krylov space the chain can exhaust stay on the complex128 path (same Philox
+  // start vectors), where the reference's breakdown test is meaningful.
+  if (dim <= 2 * static_cast<int64_t>(M)) return ftlm_gpu_ftlm_sector(s, bts, n_bt, R, M, seed, FTLM_START_PHILOX, lnz, energy);
+  if (s->plan.max_up_deg > 120)
+    return fail(FTLM_ERR_UNSUPPORTED, "batched path: more than 120 up-hop sources per string");
+  std::vector<double> A, B;
+  std::vector<int> used;
+  rc = bt_run_chains(s, R, M, seed, &A, &B, &used);
+  if (rc) return rc;
+  std::vector<double> lq(static_cast<size_t>(R) * n_bt), eq(static_cast<size_t>(R) * n_bt);
+  rc = ftlm_gpu_tridiag_quadrature(A.data(), B.data(), used.data(), R, M, bts, n_bt, lq.data(), eq.data());
+  if (rc) return rc;
+  return ftlm_gpu_ftlm_combine(lq.data(), eq.data(), used.data(), R, n_bt, std::log(static_cast<double>(dim)), lnz, energy);
+}
+
+int ftlm_gpu_batched_sweep(const ftlm_params* p, int R, int M, unsigned seed, const double* bts, int n_bt,
+                           const double* mus, int n_mu, double* lnz_s, double* e_s, double* lnz_gc, double* n_avg,
+                           double* e_avg) {
+  if (!p || !lnz_s || !e_s) return fail(FTLM_ERR_INVALID, "null argument");
+  const int n = p->Lx * p->Ly;
+  if (n <= 0 || n > 32) return fail(FTLM_ERR_INVALID, "FockBasis: require 1 <= n_sites <= 32 (bit packing)");
+  const int nsec = (n + 1) * (n + 1);
+  std::vector<int> N(static_cast<size_t>(nsec));
+  for (int nu = 0; nu <= n; ++nu)
+    for (int nd = 0; nd <= n; ++nd) {
+      const int idx = nu * (n + 1) + nd;
+      N[static_cast<size_t>(idx)] = nu + nd;
+      ftlm_sector* s = nullptr;
+      int rc = ftlm_gpu_sector_create(p, nu, nd, &s);
+      if (rc) return rc;
+      rc = ftlm_gpu_batched_ftlm_sector(s, bts, n_bt, R, M, seed, lnz_s + static_cast<size_t>(idx) * n_bt,
+                                        e_s + static_cast<size_t>(idx) * n_bt);
+      ftlm_gpu_sector_destroy(s);
+      if (rc) return rc;
+    }
+  if (lnz_gc && n_avg && e_avg)
+    return ftlm_gpu_gc_reduce(lnz_s, e_s, N.data(), nsec, bts, n_bt, mus, n_mu, n, lnz_gc, n_avg, e_avg);
+  return FTLM_OK;
+}
+
+int ftlm_gpu_batched_release(void) {
+  std::lock_guard<std::mutex> lock(g_bt_mu);
+  g_bt.release();
   return FTLM_OK;
 }
 

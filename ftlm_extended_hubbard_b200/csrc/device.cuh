@@ -21,6 +21,10 @@ struct DevSector {
   const uint32_t* up_lohi; // [nnz_up]
   const int64_t* dn_gptr;  // [ngroups+1]
   const uint32_t* dn_ent;  // ELL entries
+  const int64_t* dn_csr_ptr;   // [Dd+1] unpadded down-hop lists (batched path)
+  const uint32_t* dn_csr_ent;
+  const float2* up_coef32;     // [nnz_up] complex64 copies for the batched path
+  const float2* dn_coef32;     // [n_dn_hops+1]
   const double2* dn_coef;  // [n_dn_hops+1]
   const uint32_t* dn_nmask;// [n_dn_hops+1]
   int n_dn_hops;           // == pad hop id

@@ -286,7 +286,7 @@ std::string build_plan(int n_sites, int n_up, int n_dn, double U, double V, cons
   P.dim = P.up.D * P.dn.D;
   P.hu = merge_hops(hops, 0);
   P.hd = merge_hops(hops, 1);
-  if (P.hd.size() + 1 > 511) return "more than 510 distinct down hoppings are not supported";
+  if (P.hd.size() + 1 > 256) return "more than 255 distinct down hoppings are not supported";
 
   // Diagonal tables.  sum_pairs (u_i+d_i)(u_j+d_j) = uu + dd + sum_s d_s * c_u(s).
   P.cnt_uu.resize(static_cast<size_t>(P.up.D));
@@ -352,6 +352,7 @@ std::string build_plan(int n_sites, int n_up, int n_dn, double U, double V, cons
   }
   const int64_t ngroups = (P.dn.D + 31) / 32;
   P.dn_gptr.assign(static_cast<size_t>(ngroups) + 1, 0);
+  P.dn_csr_ptr.assign(static_cast<size_t>(P.dn.D) + 1, 0);
   std::vector<std::vector<uint32_t>> lane(32);
   std::vector<std::vector<uint32_t>> sched(32);
   int64_t total_src = 0;
@@ -373,6 +374,10 @@ std::string build_plan(int n_sites, int n_up, int n_dn, double U, double V, cons
       }
       total_src += static_cast<int64_t>(lane[l].size());
       P.max_dn_deg = std::max(P.max_dn_deg, static_cast<int>(lane[l].size()));
+      for (uint32_t en : lane[l]) P.dn_csr_ent.push_back(((en >> 10) << 9) | (((en >> 1) & 511u) << 1) | (en & 1u));
+      while ((P.dn_csr_ent.size() - static_cast<size_t>(P.dn_csr_ptr[static_cast<size_t>(r)])) % 8 != 0)
+        P.dn_csr_ent.push_back((static_cast<uint32_t>(r) << 9) | (static_cast<uint32_t>(P.dn_pad_hop) << 1));
+      P.dn_csr_ptr[static_cast<size_t>(r) + 1] = static_cast<int64_t>(P.dn_csr_ent.size());
     }
     // Per quarter-warp (8 lanes), order the entries so that in every round the 8 lanes read
     // 8 different shared-memory bank groups (a 16-byte element src sits in group src % 8).

@@ -75,6 +75,10 @@ struct SectorPlan {
   std::vector<int64_t> dn_gptr;
   std::vector<uint32_t> dn_ent;
   int dn_pad_hop = 0;
+  // Batched path: per output down string, entries src<<9 | (2*hop_id + sign), padded to a multiple
+  // of 8 with (self, pad hop) entries: dn_csr_ptr[Dd+1], dn_csr_ent.
+  std::vector<int64_t> dn_csr_ptr;
+  std::vector<uint32_t> dn_csr_ent;
   std::vector<double> dn_coef;     // 2 per hop id (pad hop id has 0)
   std::vector<uint32_t> dn_nmask;  // per hop id
 

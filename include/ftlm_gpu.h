@@ -172,6 +172,24 @@ int ftlm_gpu_gc_sweep(const ftlm_params* p, int R, int M, unsigned seed, int sta
                       const double* mus, int n_mu, double* lnz_s, double* e_s, double* lnz_gc, double* n_avg,
                       double* e_avg);
 
+/* ---- batched complex64 FTLM (32 chains of a sector per block vector, FP64 scalars) ----
+ * Chain r of a sector uses the Philox start vector of FTLM_START_PHILOX with seed + r*100003 (the
+ * same vectors the complex128 path draws), rounded to complex64; H·v in FP32, dot products and
+ * norms in compensated FP64; the M steps of each 32-chain block run as one CUDA graph.  Device
+ * memory: 3 block vectors of dim*32 complex64 (127 GB at 4x4 (8,8)), kept between calls until
+ * ftlm_gpu_batched_release(). */
+/* alpha/beta [R][M] (beta zero-padded after a breakdown), used [R]. */
+int ftlm_gpu_batched_lanczos(ftlm_sector* s, int R, int M, unsigned seed, double* alpha, double* beta, int* used);
+/* ftlm_gpu_ftlm_sector on the batched path; sectors with dim <= 2M use the complex128 path with
+ * FTLM_START_PHILOX (their Krylov space can be exhausted, where FP64 breakdown detection matters). */
+int ftlm_gpu_batched_ftlm_sector(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed, double* lnz,
+                                 double* energy);
+/* ftlm_gpu_gc_sweep on the batched path (config: all sectors, R chains, M steps). */
+int ftlm_gpu_batched_sweep(const ftlm_params* p, int R, int M, unsigned seed, const double* bts, int n_bt,
+                           const double* mus, int n_mu, double* lnz_s, double* e_s, double* lnz_gc, double* n_avg,
+                           double* e_avg);
+int ftlm_gpu_batched_release(void);
+
 #ifdef __cplusplus
 }
 #endif
