@@ -282,6 +282,77 @@ class Sector(_Handle):
         return lnz, en
 
 
+    def orbit_block(self, kx: int, ky: int) -> "OrbitKBlock":
+        return OrbitKBlock(self, kx, ky)
+
+    def orbit_ftlm(self, betas, n_random: int, lanczos_steps: int, seed: int, sector_index: int = 0,
+                   start: str = "reference"):
+        """k-resolved sector ln Z: every momentum block with seed + sector_index*257 + ky*17 + kx,
+        log-sum-exp over blocks.  Returns (lnz, energy, block dims [Ly][Lx])."""
+        bt = np.ascontiguousarray(np.atleast_1d(np.asarray(betas, dtype=np.float64)))
+        lnz = np.zeros(bt.size)
+        en = np.zeros(bt.size)
+        Lx, Ly = (self.params.Lx, self.params.Ly) if self.params is not None else (0, 0)
+        dims = np.zeros(max(1, Lx * Ly), np.int64)
+        call("ftlm_gpu_orbit_sector_ftlm", self._h, bt.ctypes.data_as(C.c_void_p), bt.size, n_random, lanczos_steps,
+             C.c_uint(seed & 0xFFFFFFFF), sector_index, START_MODES[start], lnz.ctypes.data_as(C.c_void_p),
+             en.ctypes.data_as(C.c_void_p), dims.ctypes.data_as(C.c_void_p))
+        return lnz, en, dims[:Lx * Ly].reshape(Ly, Lx)
+
+
+class OrbitKBlock:
+    """Translation-orbit momentum block K = (kx, ky) of a sector (OrbitKBlockBasis + apply_orbit_k_block)."""
+
+    def __init__(self, sector: Sector, kx: int, ky: int):
+        self.sector = sector  # the block's device tables reference the sector's
+        self._h = C.c_void_p()
+        try:
+            call("ftlm_gpu_orbit_create", sector.handle, kx, ky, C.byref(self._h))
+        except FtlmError as e:
+            _raise_value(e)
+        d = C.c_longlong()
+        call("ftlm_gpu_orbit_dim", self._h, C.byref(d))
+        self.dim = d.value
+        self.kx, self.ky = kx, ky
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().ftlm_gpu_orbit_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def entries(self):
+        """Packed representatives (up<<16 | dn) and |A(K)|, ascending packed order."""
+        rep = np.zeros(max(1, self.dim), np.uint32)
+        absA = np.zeros(max(1, self.dim))
+        call("ftlm_gpu_orbit_entries", self._h, rep.ctypes.data_as(C.c_void_p), absA.ctypes.data_as(C.c_void_p))
+        return rep[:self.dim], absA[:self.dim]
+
+    def apply(self, x, y, stream: int = 0):
+        call("ftlm_gpu_orbit_apply", self._h, C.c_void_p(_ptr(x)), C.c_void_p(_ptr(y)), C.c_void_p(stream))
+
+    def apply_host(self, x: np.ndarray, y: Optional[np.ndarray] = None) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.complex128)
+        if y is None:
+            y = np.empty_like(x)
+        call("ftlm_gpu_orbit_apply_host", self._h, x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p))
+        return y
+
+    def ftlm(self, betas, n_random: int, lanczos_steps: int, seed: int, start: str = "reference"):
+        bt = np.ascontiguousarray(np.atleast_1d(np.asarray(betas, dtype=np.float64)))
+        lnz = np.zeros(bt.size)
+        en = np.zeros(bt.size)
+        call("ftlm_gpu_orbit_ftlm", self._h, bt.ctypes.data_as(C.c_void_p), bt.size, n_random, lanczos_steps,
+             C.c_uint(seed & 0xFFFFFFFF), START_MODES[start], lnz.ctypes.data_as(C.c_void_p),
+             en.ctypes.data_as(C.c_void_p))
+        return lnz, en
+
+
 @dataclass
 class LanczosExtrema:
     min_eval: float = 0.0

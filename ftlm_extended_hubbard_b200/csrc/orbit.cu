@@ -1,0 +1,195 @@
+// Translation-orbit k-block kernels; conventions in orbit.cuh.
+//
+// Canonical representative = the translation image with the smallest packed (up<<16 | dn)
+// (include/ftlm/symmetry/orbit.hpp:115-119).  For a state s, R is the first translation in the
+// reference's search order (dx outer, dy inner; src/orbit_k_block_basis.cpp:225-236) with
+// T_R rep = s, and eta = (-1)^(inversions of the occupied modes 2*site+spin, listed in site order,
+// after translation) (include/ftlm/symmetry/fermionic_translation.hpp:32-54).
+#include "orbit.cuh"
+
+namespace ftlm_b200 {
+
+namespace {
+
+__device__ __forceinline__ uint32_t translate(const OrbitDev& O, int R, uint32_t m) {
+  const uint16_t* t = O.tlut + R * 512;
+  return static_cast<uint32_t>(t[m & 255u]) | static_cast<uint32_t>(t[256 + (m >> 8)]);
+}
+
+// Parity of the inversions of T_R on the occupied modes of (u, d).
+__device__ __forceinline__ uint32_t translation_sign(const OrbitDev& O, int R, uint32_t u, uint32_t d) {
+  const uint8_t* ts = O.tsite + R * 16;
+  uint64_t seen = 0;
+  uint32_t inv = 0;
+  for (int s = 0; s < O.n; ++s) {
+    const uint32_t tsite = ts[s];
+    if ((u >> s) & 1u) {
+      const uint32_t tm = 2u * tsite;
+      inv += __popcll(seen >> (tm + 1));
+      seen |= 1ull << tm;
+    }
+    if ((d >> s) & 1u) {
+      const uint32_t tm = 2u * tsite + 1u;
+      inv += __popcll(seen >> (tm + 1));
+      seen |= 1ull << tm;
+    }
+  }
+  return inv & 1u;
+}
+
+__global__ void canon_kernel(OrbitDev O, int32_t* __restrict__ rep_full, uint8_t* __restrict__ reta) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < O.dim; i += stride) {
+    const int64_t ru = i / O.Dd;
+    const uint32_t u = O.umask[ru], d = O.dmask[i - ru * O.Dd];
+    uint32_t best = (u << 16) | d;
+    for (int R = 1; R < O.G; ++R) {
+      const uint32_t p = (translate(O, R, u) << 16) | translate(O, R, d);
+      best = min(best, p);
+    }
+    const uint32_t bu = best >> 16, bd = best & 0xFFFFu;
+    int Rf = 0;
+    for (int k = 0; k < O.G; ++k) {
+      const int R = O.rorder[k];
+      if (translate(O, R, bu) == u && translate(O, R, bd) == d) {
+        Rf = R;
+        break;
+      }
+    }
+    rep_full[i] = static_cast<int32_t>(static_cast<int64_t>(O.rank_u[bu]) * O.Dd + O.rank_d[bd]);
+    reta[i] = static_cast<uint8_t>(Rf | (translation_sign(O, Rf, bu, bd) << 4));
+  }
+}
+
+__global__ void absA_kernel(OrbitDev O, const uint32_t* __restrict__ reps, int64_t nreps,
+                            const double2* __restrict__ chi_tab, double* __restrict__ absA) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t b = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; b < nreps; b += stride) {
+    const uint32_t u = reps[b] >> 16, d = reps[b] & 0xFFFFu;
+    double ar = 0.0, ai = 0.0;
+    for (int R = 0; R < O.G; ++R) {  // dy outer, dx inner: R = dy * Lx + dx ascending
+      if (translate(O, R, u) != u || translate(O, R, d) != d) continue;
+      const double eta = translation_sign(O, R, u, d) ? -1.0 : 1.0;
+      ar += eta * chi_tab[R].x;
+      ai += eta * chi_tab[R].y;
+    }
+    absA[b] = hypot(ar, ai);
+  }
+}
+
+__global__ void table_kernel(OrbitDev O, const int32_t* __restrict__ rep_full, const uint8_t* __restrict__ reta,
+                             const int32_t* __restrict__ red_of_full, uint32_t* __restrict__ table) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < O.dim; i += stride) {
+    const int32_t b = red_of_full[rep_full[i]];
+    table[i] = (b < 0) ? 0xFFFFFFFFu : (static_cast<uint32_t>(b) | (static_cast<uint32_t>(reta[i]) << 24));
+  }
+}
+
+__device__ __forceinline__ void orbit_term(const OrbitApplyDev& A, int64_t j, double2 hval, double sa,
+                                           const double2* __restrict__ x, double2& acc) {
+  const uint32_t e = A.table[j];
+  if (e == 0xFFFFFFFFu) return;
+  const uint32_t beta = e & 0xFFFFFFu;
+  const double2 xb = x[beta];
+  if (tiny(xb)) return;
+  const int R = static_cast<int>((e >> 24) & 15u);
+  const double eta = ((e >> 28) & 1u) ? -1.0 : 1.0;
+  const double2 ch = A.chi_tab[R];
+  // h * eta * chi(R) * sqrt(|A_beta| / |A_alpha|), then conjugated (gather from the Hermitian H_K)
+  const double f = eta * A.sqrtA[beta] * sa;
+  const double cr = f * (hval.x * ch.x - hval.y * ch.y);
+  const double ci = -f * (hval.x * ch.y + hval.y * ch.x);
+  acc.x = fma(cr, xb.x, acc.x);
+  acc.x = fma(-ci, xb.y, acc.x);
+  acc.y = fma(cr, xb.y, acc.y);
+  acc.y = fma(ci, xb.x, acc.y);
+}
+
+__global__ void __launch_bounds__(256) apply_kernel(OrbitApplyDev A, const double2* __restrict__ x,
+                                                    double2* __restrict__ y) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t a = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; a < A.dk; a += stride) {
+    const uint32_t u = A.reps[a] >> 16, d = A.reps[a] & 0xFFFFu;
+    const int32_t ru = A.O.rank_u[u], rd = A.O.rank_d[d];
+    double2 acc = make_double2(0.0, 0.0);
+    const double2 xa = x[a];
+    if (!tiny(xa)) {
+      const double dg = diag_value(A.S, u, d, A.S.cnt_uu[ru], A.S.cnt_dd[rd], A.S.wpl[ru]);
+      acc.x = dg * xa.x;
+      acc.y = dg * xa.y;
+    }
+    const double sa = 1.0 / A.sqrtA[a];
+    for (int h = 0; h < A.n_uhops; ++h) {
+      const int f = A.uhop_from[h], t = A.uhop_to[h];
+      if (!((u >> f) & 1u) || ((u >> t) & 1u)) continue;
+      const uint32_t u2 = u ^ (1u << f) ^ (1u << t);
+      const uint32_t neg = (__popc(u & A.uhop_own[h]) + __popc(d & A.uhop_oth[h])) & 1u;
+      double2 hv = A.uhop_c[h];
+      if (neg) hv = make_double2(-hv.x, -hv.y);
+      orbit_term(A, static_cast<int64_t>(A.O.rank_u[u2]) * A.O.Dd + rd, hv, sa, x, acc);
+    }
+    for (int h = 0; h < A.n_dhops; ++h) {
+      const int f = A.dhop_from[h], t = A.dhop_to[h];
+      if (!((d >> f) & 1u) || ((d >> t) & 1u)) continue;
+      const uint32_t d2 = d ^ (1u << f) ^ (1u << t);
+      const uint32_t neg = (__popc(d & A.dhop_own[h]) + __popc(u & A.dhop_oth[h])) & 1u;
+      double2 hv = A.dhop_c[h];
+      if (neg) hv = make_double2(-hv.x, -hv.y);
+      orbit_term(A, static_cast<int64_t>(ru) * A.O.Dd + A.O.rank_d[d2], hv, sa, x, acc);
+    }
+    y[a] = acc;
+  }
+}
+
+__global__ void scatter_kernel(const int64_t* __restrict__ full, int64_t n, int32_t* __restrict__ red) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t b = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; b < n; b += stride)
+    red[full[b]] = static_cast<int32_t>(b);
+}
+
+int g_sms = 0;
+unsigned grid_for(int64_t n) {
+  if (g_sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sms <= 0) g_sms = 148;
+  }
+  const int64_t b = (n + 255) / 256;
+  return static_cast<unsigned>(b < 16 * g_sms ? (b > 0 ? b : 1) : 16 * g_sms);
+}
+
+}  // namespace
+
+cudaError_t orbit_canon(const OrbitDev& O, int32_t* rep_full, uint8_t* reta, cudaStream_t st) {
+  canon_kernel<<<grid_for(O.dim), 256, 0, st>>>(O, rep_full, reta);
+  return cudaGetLastError();
+}
+
+cudaError_t orbit_absA(const OrbitDev& O, const uint32_t* reps, int64_t nreps, const double2* chi_tab, double* absA,
+                       cudaStream_t st) {
+  if (nreps <= 0) return cudaSuccess;
+  absA_kernel<<<grid_for(nreps), 256, 0, st>>>(O, reps, nreps, chi_tab, absA);
+  return cudaGetLastError();
+}
+
+cudaError_t orbit_table(const OrbitDev& O, const int32_t* rep_full, const uint8_t* reta, const int32_t* red_of_full,
+                        uint32_t* table, cudaStream_t st) {
+  table_kernel<<<grid_for(O.dim), 256, 0, st>>>(O, rep_full, reta, red_of_full, table);
+  return cudaGetLastError();
+}
+
+cudaError_t orbit_scatter_index(const int64_t* full, int64_t n, int32_t* red, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  scatter_kernel<<<grid_for(n), 256, 0, st>>>(full, n, red);
+  return cudaGetLastError();
+}
+
+cudaError_t orbit_apply(const OrbitApplyDev& A, const double2* x, double2* y, cudaStream_t st) {
+  if (A.dk <= 0) return cudaSuccess;
+  apply_kernel<<<grid_for(A.dk), 256, 0, st>>>(A, x, y);
+  return cudaGetLastError();
+}
+
+}  // namespace ftlm_b200

@@ -190,6 +190,27 @@ int ftlm_gpu_batched_sweep(const ftlm_params* p, int R, int M, unsigned seed, co
                            double* e_avg);
 int ftlm_gpu_batched_release(void);
 
+/* ---- translation-orbit momentum blocks (sectors built from lattice parameters, n_sites <= 16) ----
+ * Basis: canonical orbit representatives (smallest packed up<<16|dn) whose fermionic stabiliser sum
+ * |A(K)| > 1e-12, ascending packed order (OrbitKBlockBasis::build, src/orbit_k_block_basis.cpp:70-117).
+ * Apply: apply_orbit_k_block (src/orbit_k_block_basis.cpp:151-220) on reduced complex128 vectors. */
+typedef struct ftlm_orbit ftlm_orbit;
+int ftlm_gpu_orbit_create(ftlm_sector* s, int kx, int ky, ftlm_orbit** out);
+int ftlm_gpu_orbit_destroy(ftlm_orbit* o);
+int ftlm_gpu_orbit_dim(const ftlm_orbit* o, long long* dim);
+/* Host copies of the reduced basis: packed representatives and |A(K)| (OrbitKRepEntry rep / abs_A). */
+int ftlm_gpu_orbit_entries(const ftlm_orbit* o, uint32_t* rep_packed, double* absA);
+int ftlm_gpu_orbit_apply(ftlm_orbit* o, const double* x_dev, double* y_dev, void* stream);
+int ftlm_gpu_orbit_apply_host(ftlm_orbit* o, const double* x_host, double* y_host);
+/* ftlm_log_partition_complex on one block (seed_r = seed + r*100003). */
+int ftlm_gpu_orbit_ftlm(ftlm_orbit* o, const double* bts, int n_bt, int R, int M, unsigned seed, int start_mode,
+                        double* lnz, double* energy);
+/* All Lx*Ly momentum blocks of a sector with seed_k = seed + sector_index*257 + ky*17 + kx and
+ * ln Z_sector = log-sum-exp over blocks (benchmarks/bench_ftlm_nmu_4x4_k.cpp:801-1081); dims_k [Lx*Ly]
+ * (may be NULL) receives the block dimensions. */
+int ftlm_gpu_orbit_sector_ftlm(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed,
+                               int sector_index, int start_mode, double* lnz, double* energy, long long* dims_k);
+
 #ifdef __cplusplus
 }
 #endif

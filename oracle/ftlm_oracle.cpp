@@ -21,6 +21,7 @@
 #include <limits>
 #include <random>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 namespace {
@@ -412,6 +413,135 @@ double quad_energy(const double* lam, const double* w0, int n, double bT) {
   return se / s;
 }
 
+
+// ---- translation-orbit momentum blocks (reference src/orbit_k_block_basis.cpp:70-220) -----------
+// Lattice site of (x, y) is y*Lx + x; a translation by (dx, dy) sends it to
+// ((y+dy) mod Ly)*Lx + (x+dx) mod Lx (include/ftlm/symmetry/occup_bits_translate.hpp:10-27).
+int shifted_site(int site, int Lx, int Ly, int dx, int dy) {
+  return ((site / Lx + dy) % Ly) * Lx + (site % Lx + dx) % Lx;
+}
+
+uint32_t shift_bits(uint32_t m, int Lx, int Ly, int dx, int dy) {
+  uint32_t out = 0;
+  for (int site = 0; site < Lx * Ly; ++site)
+    if ((m >> site) & 1u) out |= 1u << shifted_site(site, Lx, Ly, dx, dy);
+  return out;
+}
+
+uint32_t pack(uint32_t u, uint32_t d) { return (u << 16) | d; }
+
+// include/ftlm/symmetry/fermionic_translation.hpp:32-54 — (-1)^(inversions) of the occupied modes
+// 2*site+spin listed in site order (up before down), each sent through the translation.
+double shift_sign(uint32_t u, uint32_t d, int Lx, int Ly, int dx, int dy) {
+  std::vector<int> modes;
+  for (int site = 0; site < Lx * Ly; ++site) {
+    const int ts = shifted_site(site, Lx, Ly, dx, dy);
+    if ((u >> site) & 1u) modes.push_back(2 * ts);
+    if ((d >> site) & 1u) modes.push_back(2 * ts + 1);
+  }
+  int inv = 0;
+  for (size_t i = 0; i < modes.size(); ++i)
+    for (size_t j = i + 1; j < modes.size(); ++j) inv += modes[i] > modes[j] ? 1 : 0;
+  return (inv & 1) ? -1.0 : 1.0;
+}
+
+// include/ftlm/symmetry/orbit.hpp:115-119 — smallest packed image over the translation group.
+uint32_t orbit_min(uint32_t u, uint32_t d, int Lx, int Ly) {
+  uint32_t best = pack(u, d);
+  for (int dy = 0; dy < Ly; ++dy)
+    for (int dx = 0; dx < Lx; ++dx)
+      best = std::min(best, pack(shift_bits(u, Lx, Ly, dx, dy), shift_bits(d, Lx, Ly, dx, dy)));
+  return best;
+}
+
+// include/ftlm/symmetry/momentum_sector.hpp:57-63 — chi_K^*(R) = exp(-2 pi i (kx dx/Lx + ky dy/Ly)).
+cd bloch(int kx, int ky, int Lx, int Ly, int dx, int dy) {
+  const double pi = std::acos(-1.0);
+  const double th = -2.0 * pi *
+                    (static_cast<double>(kx * dx) / static_cast<double>(Lx) +
+                     static_cast<double>(ky * dy) / static_cast<double>(Ly));
+  return {std::cos(th), std::sin(th)};
+}
+
+struct OrbitBlock {
+  const Sector* s;
+  int kx, ky;
+  std::vector<uint32_t> reps;  // surviving representatives, ascending packed
+  std::vector<double> absA;
+  std::vector<int> size;       // orbit size
+  std::unordered_map<uint32_t, int> row;
+};
+
+// src/orbit_k_block_basis.cpp:70-117 — distinct canonical representatives of the sector; stabiliser
+// sum A = sum_{R in Stab} eta(rep, R) chi_K^*(R) over R in (dy outer, dx inner) order
+// (include/ftlm/symmetry/translation_group.hpp:23-29); keep |A| > 1e-12.
+OrbitBlock* make_orbit(const Sector* s, int kx, int ky) {
+  if (s->n > 16) return nullptr;
+  const int Lx = s->Lx, Ly = s->Ly;
+  std::vector<uint32_t> all;
+  for (long long i = 0; i < s->dim(); ++i)
+    all.push_back(orbit_min(static_cast<uint32_t>(s->up_of(i)), static_cast<uint32_t>(s->dn_of(i)), Lx, Ly));
+  std::sort(all.begin(), all.end());
+  all.erase(std::unique(all.begin(), all.end()), all.end());
+  auto* o = new OrbitBlock{s, kx, ky, {}, {}, {}, {}};
+  for (uint32_t p : all) {
+    const uint32_t u = p >> 16, d = p & 0xFFFFu;
+    cd A(0.0, 0.0);
+    int stab = 0;
+    for (int dy = 0; dy < Ly; ++dy)
+      for (int dx = 0; dx < Lx; ++dx) {
+        if (shift_bits(u, Lx, Ly, dx, dy) != u || shift_bits(d, Lx, Ly, dx, dy) != d) continue;
+        ++stab;
+        A += cd(shift_sign(u, d, Lx, Ly, dx, dy), 0.0) * bloch(kx, ky, Lx, Ly, dx, dy);
+      }
+    const double a = std::abs(A);
+    if (a <= 1e-12) continue;
+    o->row[p] = static_cast<int>(o->reps.size());
+    o->reps.push_back(p);
+    o->absA.push_back(a);
+    o->size.push_back(Lx * Ly / stab);
+  }
+  return o;
+}
+
+// src/orbit_k_block_basis.cpp:151-220 — scatter over source representatives beta (skipping
+// |x_beta|^2 < 1e-28): diagonal, then every hop of rep(beta) in list order to s'; s' = T_R rep(alpha)
+// with R the first translation in (dx outer, dy inner) order (:127-149);
+// y_alpha += h * (eta * sqrt(|A_alpha|/|A_beta|)) * chi_K^*(R) * x_beta.
+void orbit_apply(const OrbitBlock& o, const cd* x, cd* y) {
+  const Sector& s = *o.s;
+  const int Lx = s.Lx, Ly = s.Ly;
+  const size_t dk = o.reps.size();
+  std::fill(y, y + dk, cd(0.0, 0.0));
+  for (size_t b = 0; b < dk; ++b) {
+    const cd xb = x[b];
+    if (std::norm(xb) < 1e-28) continue;
+    const uint32_t u = o.reps[b] >> 16, d = o.reps[b] & 0xFFFFu;
+    y[b] += cd(s.diag(u, d), 0.0) * xb;
+    for (const auto& h : s.hops) {
+      const uint32_t occ = h.spin == 0 ? u : d;
+      if (!((occ >> h.from) & 1u) || ((occ >> h.to) & 1u)) continue;
+      const uint32_t flip = (1u << h.from) | (1u << h.to);
+      const uint32_t u2 = h.spin == 0 ? u ^ flip : u, d2 = h.spin == 0 ? d : d ^ flip;
+      const double jw = (between(2 * h.from + h.spin, 2 * h.to + h.spin, u, d) & 1) ? -1.0 : 1.0;
+      const cd hv = jw * h.coeff;
+      const auto it = o.row.find(orbit_min(u2, d2, Lx, Ly));
+      if (it == o.row.end()) continue;
+      const int a = it->second;
+      const uint32_t ru = o.reps[static_cast<size_t>(a)] >> 16, rd = o.reps[static_cast<size_t>(a)] & 0xFFFFu;
+      for (int dx = 0, done = 0; dx < Lx && !done; ++dx)
+        for (int dy = 0; dy < Ly; ++dy) {
+          if (shift_bits(ru, Lx, Ly, dx, dy) != u2 || shift_bits(rd, Lx, Ly, dx, dy) != d2) continue;
+          const double eta = shift_sign(ru, rd, Lx, Ly, dx, dy);
+          const double nrm = std::sqrt(o.absA[static_cast<size_t>(a)] / o.absA[b]);
+          y[static_cast<size_t>(a)] += hv * cd(eta * nrm, 0.0) * bloch(o.kx, o.ky, Lx, Ly, dx, dy) * xb;
+          done = 1;
+          break;
+        }
+    }
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -556,15 +686,18 @@ int or_sector_lanczos_extrema(void* h, int M, unsigned seed, double* mn, double*
   return used;
 }
 
+}  // extern "C"
+
+namespace {
+
 // src/ftlm_thermo.cpp:213-256 — ln Tr e^{-bT H} for one sector, evaluated at n_bt temperatures
 // from the same R chains (the reference re-runs the chains per temperature; the chains do not
 // depend on the temperature, so the values are identical).  seed_r = seed + r*100003.
 // Outputs: lnz[n_bt], energy[n_bt] (FTLM estimate of <H>_sector), lam/w0 per chain if non-null
 // (R*M each, padded with w=0).
-void or_sector_ftlm(void* h, const double* bts, int n_bt, int R, int M, unsigned seed, int mode, int nthreads,
-                    double* lnz, double* energy, double* lam_out, double* w_out, int* used_out) {
-  auto* s = static_cast<Sector*>(h);
-  const long long dim = s->dim();
+template <class Apply>
+void ftlm_core(long long dim, Apply&& apply_h, double h00, const double* bts, int n_bt, int R, int M, unsigned seed,
+               double* lnz, double* energy, double* lam_out, double* w_out, int* used_out) {
   R = std::max(1, R);
   M = std::max(1, M);
   if (dim <= 0) {
@@ -575,7 +708,6 @@ void or_sector_ftlm(void* h, const double* bts, int n_bt, int R, int M, unsigned
     return;
   }
   if (dim == 1) {  // src/ftlm_thermo.cpp:219-223
-    const double h00 = s->diag(s->up_of(0), s->dn_of(0));
     for (int b = 0; b < n_bt; ++b) {
       lnz[b] = -bts[b] * h00;
       energy[b] = h00;
@@ -594,7 +726,7 @@ void or_sector_ftlm(void* h, const double* bts, int n_bt, int R, int M, unsigned
   for (int r = 0; r < R; ++r) {
     std::vector<double> a, b;
     const unsigned seed_r = seed + static_cast<unsigned>(r) * 100003u;
-    used[r] = lanczos(dim, [&](const cd* x, cd* y) { apply_mode(*s, x, y, mode, nthreads); }, M, seed_r, &a, &b);
+    used[r] = lanczos(dim, apply_h, M, seed_r, &a, &b);
     if (used[r] <= 0) continue;
     const int n = static_cast<int>(a.size());
     lams[r].resize(static_cast<size_t>(n));
@@ -636,6 +768,19 @@ void or_sector_ftlm(void* h, const double* bts, int n_bt, int R, int M, unsigned
   }
 }
 
+}  // namespace
+
+extern "C" {
+
+void or_sector_ftlm(void* h, const double* bts, int n_bt, int R, int M, unsigned seed, int mode, int nthreads,
+                    double* lnz, double* energy, double* lam_out, double* w_out, int* used_out) {
+  auto* s = static_cast<Sector*>(h);
+  const double h00 = s->dim() == 1 ? s->diag(s->up_of(0), s->dn_of(0)) : 0.0;
+  ftlm_core(
+      s->dim(), [&](const cd* x, cd* y) { apply_mode(*s, x, y, mode, nthreads); }, h00, bts, n_bt, R, M, seed, lnz,
+      energy, lam_out, w_out, used_out);
+}
+
 // benchmarks/bench_ftlm_nmu_rect.cpp:186-219 — grand-canonical combination of sector ln Z_s
 // over a (beta, mu) grid: ln Z_GC = LSE_s(ln Z_s + beta mu N_s); <n> = <N>/n_sites;
 // <E> = sum_s w_s E_s / sum_s w_s.  lnz_s/e_s are [n_sec][n_bt]; outputs [n_bt][n_mu].
@@ -672,6 +817,36 @@ void or_gc_reduce(const double* lnz_s, const double* e_s, const int* N_s, int n_
       e_avg[o] = (sw > 0.0) ? sew / sw : 0.0;
     }
   }
+}
+
+// Orbit momentum block of a sector (n_sites <= 16); NULL when unsupported.
+void* or_orbit_create(void* sector, int kx, int ky) { return make_orbit(static_cast<Sector*>(sector), kx, ky); }
+void or_orbit_destroy(void* h) { delete static_cast<OrbitBlock*>(h); }
+long long or_orbit_dim(void* h) { return static_cast<long long>(static_cast<OrbitBlock*>(h)->reps.size()); }
+void or_orbit_entries(void* h, uint32_t* rep, double* absA, int* orbit_size) {
+  const auto* o = static_cast<OrbitBlock*>(h);
+  for (size_t i = 0; i < o->reps.size(); ++i) {
+    if (rep) rep[i] = o->reps[i];
+    if (absA) absA[i] = o->absA[i];
+    if (orbit_size) orbit_size[i] = o->size[i];
+  }
+}
+void or_orbit_apply(void* h, const double* x, double* y) {
+  orbit_apply(*static_cast<OrbitBlock*>(h), reinterpret_cast<const cd*>(x), reinterpret_cast<cd*>(y));
+}
+// ftlm_log_partition_complex on the block (seed_r = seed + r*100003), at n_bt temperatures.
+void or_orbit_ftlm(void* h, const double* bts, int n_bt, int R, int M, unsigned seed, double* lnz, double* energy) {
+  auto* o = static_cast<OrbitBlock*>(h);
+  const long long dk = static_cast<long long>(o->reps.size());
+  double h00 = 0.0;
+  if (dk == 1) {
+    cd one(1.0, 0.0), y0;
+    orbit_apply(*o, &one, &y0);
+    h00 = y0.real();
+  }
+  ftlm_core(
+      dk, [&](const cd* x, cd* y) { orbit_apply(*o, x, y); }, h00, bts, n_bt, R, M, seed, lnz, energy, nullptr,
+      nullptr, nullptr);
 }
 
 }  // extern "C"

@@ -66,6 +66,14 @@ def _load_oracle() -> C.CDLL:
     L.or_geometry.argtypes = [_i, _i, _d, _d, _d, _d, _i, _vp, _vp, _vp, _vp, _i, _vp, _vp, C.POINTER(_i)]
     L.or_enumerate.restype = _ll
     L.or_enumerate.argtypes = [_i, _i, _vp]
+    L.or_orbit_create.restype = _vp
+    L.or_orbit_create.argtypes = [_vp, _i, _i]
+    L.or_orbit_destroy.argtypes = [_vp]
+    L.or_orbit_dim.restype = _ll
+    L.or_orbit_dim.argtypes = [_vp]
+    L.or_orbit_entries.argtypes = [_vp, _vp, _vp, _vp]
+    L.or_orbit_apply.argtypes = [_vp, _vp, _vp]
+    L.or_orbit_ftlm.argtypes = [_vp, _vp, _i, _i, _i, C.c_uint, _vp, _vp]
     return L
 
 
@@ -187,6 +195,43 @@ class OracleSector:
                                   P(used))
             return lnz, en, lam.reshape(R, M), w.reshape(R, M), used
         self.L.or_sector_ftlm(self.h, P(bt), bt.size, R, M, seed, mode, nthreads, P(lnz), P(en), None, None, None)
+        return lnz, en
+
+
+class OracleOrbit:
+    """In-repo restatement of one translation-orbit momentum block (OrbitKBlockBasis + apply)."""
+
+    def __init__(self, sector: OracleSector, kx: int, ky: int):
+        self.L = sector.L
+        self.sector = sector  # keeps the sector alive
+        self.h = self.L.or_orbit_create(sector.h, kx, ky)
+        if not self.h:
+            raise ValueError("orbit blocks need n_sites <= 16")
+        self.dim = self.L.or_orbit_dim(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.or_orbit_destroy(self.h)
+            self.h = None
+
+    def entries(self):
+        rep = np.zeros(self.dim, np.uint32)
+        absA = np.zeros(self.dim)
+        size = np.zeros(self.dim, np.int32)
+        self.L.or_orbit_entries(self.h, P(rep), P(absA), P(size))
+        return rep, absA, size
+
+    def apply(self, x):
+        x = np.ascontiguousarray(x, np.complex128)
+        y = np.zeros_like(x)
+        self.L.or_orbit_apply(self.h, P(x), P(y))
+        return y
+
+    def ftlm(self, betas, R, M, seed):
+        bt = np.ascontiguousarray(np.atleast_1d(betas), np.float64)
+        lnz = np.zeros(bt.size)
+        en = np.zeros(bt.size)
+        self.L.or_orbit_ftlm(self.h, P(bt), bt.size, R, M, seed, P(lnz), P(en))
         return lnz, en
 
 

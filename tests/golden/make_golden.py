@@ -7,6 +7,9 @@ published_tsv.npz  the reference's own published n(mu) tables (benchmarks/data/*
                    3x2 from the non-momentum solver; plus the per-sector ln Z lines of the 3x2 run log.
 ref_small.npz      outputs of the reference library itself (oracle/_ref): H·x on seeded vectors,
                    Lanczos alpha/beta, lanczos_extrema, and sector ln Z for small sectors.
+orbit_small.npz    translation-orbit momentum blocks from the reference library (OrbitKBlockBasis::build,
+                   apply_orbit_k_block, ftlm_log_partition_complex): representatives, |A|, orbit sizes,
+                   H_K x on seeded vectors and block ln Z.
 config0_4x2.npz    the plain FTLM sweep of 4x2, t=1 t'=-0.25 U=8 V=1, phi=0, R=20, M=60, seed 7,
                    T = 0.1..2.0 (20) x mu = -4..8 (49), computed by the oracle in the reference's
                    scatter order (bit-identical to the reference library; this script checks the
@@ -120,6 +123,47 @@ def ref_small():
     return out
 
 
+ORBIT_CASES = [
+    # Lx, Ly, t, tp, U, V, phix, phiy, nu, nd, kx, ky
+    (2, 2, 1.0, 0.0, 4.0, 0.5, 0.0, 0.0, 2, 2, 0, 0),
+    (2, 2, 1.0, 0.0, 4.0, 0.5, 0.0, 0.0, 2, 2, 1, 1),
+    (3, 2, 1.0, -0.35, 5.75, 0.9, 0.0, 0.0, 2, 3, 1, 0),
+    (3, 2, 1.0, -0.35, 5.75, 0.9, 0.0, 0.0, 3, 3, 1, 0),
+    (4, 2, 1.0, -0.25, 8.0, 1.0, 0.0, 0.0, 3, 3, 2, 1),
+    (3, 3, 1.0, -0.25, 6.0, 0.5, 0.0, 0.0, 2, 2, 1, 2),
+    (4, 3, 1.0, -0.25, 6.0, 0.5, 0.0, 0.0, 2, 1, 3, 2),
+    (4, 4, 1.0, -0.25, 6.0, 0.5, 0.0, 0.0, 2, 1, 1, 3),
+]
+
+
+def orbit_small():
+    R = O.reference()
+    assert R is not None, "reference library unavailable"
+    out = {"cases": np.array(ORBIT_CASES, dtype=np.float64)}
+    rng = np.random.default_rng(20240602)
+    for k, c in enumerate(ORBIT_CASES):
+        h = R.ref_sector_create(*c[:10])
+        o = R.ref_orbit_create(h, c[10], c[11])
+        dk = R.ref_orbit_dim(o)
+        rep = np.zeros(dk, np.uint32)
+        absA = np.zeros(dk)
+        size = np.zeros(dk, np.int32)
+        R.ref_orbit_entries(o, O.P(rep), O.P(absA), O.P(size))
+        x = rng.standard_normal(dk) + 1j * rng.standard_normal(dk)
+        x[rng.random(dk) < 0.05] = 0.0
+        y = np.zeros(dk, np.complex128)
+        R.ref_orbit_apply(o, O.P(x), O.P(y))
+        out[f"rep{k}"] = rep
+        out[f"absA{k}"] = absA
+        out[f"size{k}"] = size
+        out[f"x{k}"] = x
+        out[f"y{k}"] = y
+        out[f"lnz{k}"] = np.array([R.ref_orbit_ftlm_complex(o, 1.3, 5, 30, 17 + k)])
+        R.ref_orbit_destroy(o)
+        R.ref_sector_destroy(h)
+    return out
+
+
 CONFIG0 = dict(Lx=4, Ly=2, t=1.0, tp=-0.25, U=8.0, V=1.0, phix=0.0, phiy=0.0, R=20, M=60, seed=7)
 T_GRID = np.round(np.arange(1, 21) * 0.1, 10)
 MU_GRID = np.round(np.arange(49) * 0.25 - 4.0, 10)
@@ -150,6 +194,7 @@ def main():
     O.build(ref=True)
     np.savez_compressed(os.path.join(HERE, "published_tsv.npz"), **published())
     np.savez_compressed(os.path.join(HERE, "ref_small.npz"), **ref_small())
+    np.savez_compressed(os.path.join(HERE, "orbit_small.npz"), **orbit_small())
     np.savez_compressed(os.path.join(HERE, "config0_4x2.npz"), **config0())
     print("wrote", os.listdir(HERE))
 

@@ -156,3 +156,101 @@ def test_config0_golden_is_self_consistent(golden):
     # dims are the binomial products of the 4x2 sectors
     from math import comb
     assert [int(d) for d in g["dims"]] == [comb(8, a) * comb(8, b) for a in range(9) for b in range(9)]
+
+
+# ---- translation-orbit momentum blocks ----------------------------------------------------------
+ORBIT_CASES = [
+    # Lx, Ly, t, tp, U, V, phix, phiy, nu, nd, K list
+    ((2, 2, 1.0, 0.0, 4.0, 0.5, 0.0, 0.0, 2, 2), [(0, 0), (1, 0), (0, 1), (1, 1)]),
+    ((2, 2, 1.0, -0.35, 5.75, 0.9, 0.0, 0.0, 1, 1), [(0, 0), (1, 1)]),
+    ((3, 2, 1.0, -0.35, 5.75, 0.9, 0.0, 0.0, 2, 3), [(1, 0), (2, 1)]),
+    ((3, 2, 1.0, -0.35, 5.75, 0.9, 0.0, 0.0, 3, 3), [(1, 0)]),
+    ((4, 2, 1.0, -0.25, 8.0, 1.0, 0.0, 0.0, 3, 3), [(0, 0), (2, 1), (3, 0)]),
+    ((3, 3, 1.0, -0.25, 6.0, 0.5, 0.0, 0.0, 2, 2), [(0, 0), (1, 2)]),
+    ((4, 3, 1.0, -0.25, 6.0, 0.5, 0.0, 0.0, 2, 1), [(1, 1), (3, 2)]),
+]
+
+
+def _orbit_ids():
+    return [f"{c[0]}x{c[1]}_{c[8]}{c[9]}" for c, _ in ORBIT_CASES]
+
+
+@needs_ref
+@pytest.mark.parametrize("case", ORBIT_CASES, ids=_orbit_ids())
+def test_orbit_block_bit_exact_vs_reference(case):
+    c, ks = case
+    R = O.reference()
+    h = R.ref_sector_create(*c)
+    s = O.OracleSector(*c)
+    try:
+        for kx, ky in ks:
+            ro = R.ref_orbit_create(h, kx, ky)
+            assert ro
+            try:
+                o = O.OracleOrbit(s, kx, ky)
+                dk = R.ref_orbit_dim(ro)
+                assert dk == o.dim
+                rep = np.zeros(dk, np.uint32)
+                absA = np.zeros(dk)
+                size = np.zeros(dk, np.int32)
+                R.ref_orbit_entries(ro, O.P(rep), O.P(absA), O.P(size))
+                rep2, absA2, size2 = o.entries()
+                assert np.array_equal(rep, rep2) and np.array_equal(size, size2)
+                assert np.array_equal(absA, absA2)
+                rng = np.random.default_rng(11 + kx + 7 * ky)
+                x = rng.standard_normal(dk) + 1j * rng.standard_normal(dk)
+                x[rng.random(dk) < 0.1] = 1e-15
+                y = np.zeros(dk, np.complex128)
+                R.ref_orbit_apply(ro, O.P(x), O.P(y))
+                assert np.array_equal(o.apply(x), y)
+                if dk >= 1:
+                    lz = R.ref_orbit_ftlm_complex(ro, 0.9, 4, 20, 5)
+                    lz2, _ = o.ftlm(0.9, 4, 20, 5)
+                    assert lz == lz2[0]
+            finally:
+                R.ref_orbit_destroy(ro)
+    finally:
+        R.ref_sector_destroy(h)
+
+
+def _dense(op, n):
+    H = np.zeros((n, n), np.complex128)
+    for j in range(n):
+        e = np.zeros(n, np.complex128)
+        e[j] = 1.0
+        H[:, j] = op(e)
+    return H
+
+
+def test_orbit_known_answers():
+    """tests/test_orbit_k_block_basis.cpp:19-101: dims 12 (2x2 (2,2) Gamma) and 66 (3x2 (3,3) K=(1,0));
+    |A| = |Stab| on 2x2 Gamma; orbit sizes of the surviving reps sum to the mapped states."""
+    s = O.OracleSector(2, 2, 1.0, 0.0, 4.0, 0.5, 0.0, 0.0, 2, 2)
+    o = O.OracleOrbit(s, 0, 0)
+    assert o.dim == 12
+    _, absA, size = o.entries()
+    assert np.allclose(absA, 4.0 / size, atol=1e-9)
+    s32 = O.OracleSector(3, 2, 1.0, -0.35, 5.75, 0.9, 0.0, 0.0, 3, 3)
+    assert O.OracleOrbit(s32, 1, 0).dim == 66
+
+
+@pytest.mark.parametrize("case", ORBIT_CASES[:6], ids=_orbit_ids()[:6])
+def test_orbit_blocks_partition_spectrum(case):
+    """The momentum blocks are Hermitian and their spectra together are the sector's spectrum."""
+    c, _ = case
+    s = O.OracleSector(*c)
+    Lx, Ly = c[0], c[1]
+    ev = []
+    total = 0
+    for ky in range(Ly):
+        for kx in range(Lx):
+            o = O.OracleOrbit(s, kx, ky)
+            total += o.dim
+            if o.dim == 0:
+                continue
+            Hk = _dense(o.apply, o.dim)
+            assert np.abs(Hk - Hk.conj().T).max() < 1e-12
+            ev.append(np.linalg.eigvalsh(Hk))
+    assert total == s.dim
+    Hf = _dense(lambda v: s.apply(v, mode=0), s.dim)
+    np.testing.assert_allclose(np.sort(np.concatenate(ev)), np.linalg.eigvalsh(Hf), atol=1e-10)
