@@ -88,6 +88,7 @@ SIGNATURES = {
     "ftlm_gpu_batched_release": [],
     "ftlm_gpu_orbit_create": [_vp, _i, _i, C.POINTER(_vp)],
     "ftlm_gpu_orbit_destroy": [_vp],
+    "ftlm_gpu_orbit_set_apply_path": [_vp, _i],
     "ftlm_gpu_orbit_dim": [_vp, C.POINTER(_ll)],
     "ftlm_gpu_orbit_entries": [_vp, _vp, _vp],
     "ftlm_gpu_orbit_apply": [_vp, _vp, _vp, _vp],

@@ -326,6 +326,9 @@ class OrbitKBlock:
         except Exception:
             pass
 
+    def set_apply_path(self, path: int):
+        call("ftlm_gpu_orbit_set_apply_path", self._h, path)
+
     def entries(self):
         """Packed representatives (up<<16 | dn) and |A(K)|, ascending packed order."""
         rep = np.zeros(max(1, self.dim), np.uint32)

@@ -1003,7 +1003,7 @@ struct ftlm_orbit {
   int64_t dk = 0;
   std::vector<uint32_t> reps;  // surviving representatives (ascending packed)
   std::vector<double> absA;
-  DevBuf reps_dev, sqrtA, table, chi;
+  DevBuf reps_dev, sqrtA, table, chi, xs;
   OrbitApplyDev app{};
   LanczosWs ws;
   DevBuf hx, hy;
@@ -1214,12 +1214,21 @@ int ftlm_gpu_orbit_create(ftlm_sector* s, int kx, int ky, ftlm_orbit** out) {
   A.dhop_own = D.dh_own.as<uint32_t>();
   A.dhop_oth = D.dh_oth.as<uint32_t>();
   A.n_dhops = D.n_dh;
+  CU_TRY(o->xs.alloc(static_cast<size_t>(std::max<int64_t>(o->dk, 1)) * sizeof(double2)));
+  A.xs = o->xs.as<double2>();
+  A.path = 1;
   *out = o.release();
   return FTLM_OK;
 }
 
 int ftlm_gpu_orbit_destroy(ftlm_orbit* o) {
   delete o;
+  return FTLM_OK;
+}
+
+int ftlm_gpu_orbit_set_apply_path(ftlm_orbit* o, int path) {
+  if (!o || (path != 0 && path != 1)) return fail(FTLM_ERR_INVALID, "path must be 0 or 1");
+  o->app.path = path;
   return FTLM_OK;
 }
 

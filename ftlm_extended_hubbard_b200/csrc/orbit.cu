@@ -142,6 +142,109 @@ __global__ void __launch_bounds__(256) apply_kernel(OrbitApplyDev A, const doubl
   }
 }
 
+// sqrt(|A_b|) x_b with the reference's source-skip rule applied (a skipped source contributes
+// exactly nothing, and a zero contributes exactly nothing to the gathers below).
+__global__ void prescale_kernel(int64_t dk, const double* __restrict__ sqrtA, const double2* __restrict__ x,
+                                double2* __restrict__ xs) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t b = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; b < dk; b += stride) {
+    const double2 v = x[b];
+    const double f = sqrtA[b];
+    xs[b] = tiny(v) ? make_double2(0.0, 0.0) : make_double2(f * v.x, f * v.y);
+  }
+}
+
+// Thread per representative alpha, driven by the sector's own gather tables: the up sources of
+// rep(alpha) are the CSR row of its up string, the down sources the padded list of its down
+// string, each with the matrix element <rep alpha|H|s>.  By Hermiticity of H_K,
+//   H_K[alpha, beta] = sum_{s in orbit beta} <rep alpha|H|s> eta(beta, R_s) conj(chi(R_s)) sqrt|A_beta| / sqrt|A_alpha|,
+// so y_alpha = diag x_alpha + (1/sqrt|A_alpha|) sum <rep alpha|H|s> eta conj(chi) xs_beta.
+// Sources are taken four at a time: four table lookups, then four gathers of xs, in flight together.
+constexpr int kOrbBatch = 4;
+
+__device__ __forceinline__ void orbit_acc(double2 c, uint32_t e, double2 xb, double2& acc, const double2* chi) {
+  const double2 ch = chi[(e >> 24) & 15u];
+  const double eta = ((e >> 28) & 1u) ? -1.0 : 1.0;
+  const double cr = eta * (c.x * ch.x + c.y * ch.y);
+  const double ci = eta * (c.y * ch.x - c.x * ch.y);
+  acc.x = fma(cr, xb.x, acc.x);
+  acc.x = fma(-ci, xb.y, acc.x);
+  acc.y = fma(cr, xb.y, acc.y);
+  acc.y = fma(ci, xb.x, acc.y);
+}
+
+__global__ void __launch_bounds__(256) apply_tables_kernel(OrbitApplyDev A, const double2* __restrict__ x,
+                                                           double2* __restrict__ y) {
+  const DevSector& S = A.S;
+  const int64_t Dd = A.O.Dd;
+  const double2* __restrict__ xs = A.xs;
+  const uint32_t* __restrict__ table = A.table;
+  constexpr uint32_t kNone = 0xFFFFFFFFu;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t a = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; a < A.dk; a += stride) {
+    const uint32_t pk = A.reps[a];
+    const uint32_t u = pk >> 16, d = pk & 0xFFFFu;
+    const int32_t ru = A.O.rank_u[u], rd = A.O.rank_d[d];
+    double2 acc = make_double2(0.0, 0.0);
+    // up sources: same down string, rows up_src
+    const uint32_t q = prefix_parity_shifted(d);
+    const int p1 = S.up_ptr[ru + 1];
+    for (int p = S.up_ptr[ru]; p < p1; p += kOrbBatch) {
+      uint32_t e[kOrbBatch];
+      double2 c[kOrbBatch], xv[kOrbBatch];
+#pragma unroll
+      for (int k = 0; k < kOrbBatch; ++k) {
+        e[k] = kNone;
+        if (p + k < p1) {
+          const uint32_t lh = S.up_lohi[p + k];
+          const uint32_t neg = ((q >> (lh & 255u)) ^ (q >> (lh >> 8))) & 1u;
+          c[k] = S.up_coef[p + k];
+          if (neg) c[k] = make_double2(-c[k].x, -c[k].y);
+          e[k] = __ldg(table + static_cast<int64_t>(S.up_src[p + k]) * Dd + rd);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kOrbBatch; ++k) xv[k] = e[k] != kNone ? xs[e[k] & 0xFFFFFFu] : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < kOrbBatch; ++k)
+        if (e[k] != kNone) orbit_acc(c[k], e[k], xv[k], acc, A.chi_tab);
+    }
+    // down sources: same up string, columns from the padded down list
+    const int64_t rowbase = static_cast<int64_t>(ru) * Dd;
+    const int64_t d1 = S.dn_csr_ptr[rd + 1];
+    for (int64_t p = S.dn_csr_ptr[rd]; p < d1; p += kOrbBatch) {
+      uint32_t e[kOrbBatch];
+      double2 c[kOrbBatch], xv[kOrbBatch];
+#pragma unroll
+      for (int k = 0; k < kOrbBatch; ++k) {
+        e[k] = kNone;
+        const uint32_t ent = S.dn_csr_ent[p + k];  // lists are padded to a multiple of 8
+        const int h = static_cast<int>((ent >> 1) & 255u);
+        if (h != S.n_dn_hops) {
+          const uint32_t neg = (ent & 1u) ^ (static_cast<uint32_t>(__popc(u & S.dn_nmask[h])) & 1u);
+          c[k] = S.dn_coef[h];
+          if (neg) c[k] = make_double2(-c[k].x, -c[k].y);
+          e[k] = __ldg(table + rowbase + (ent >> 9));
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kOrbBatch; ++k) xv[k] = e[k] != kNone ? xs[e[k] & 0xFFFFFFu] : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < kOrbBatch; ++k)
+        if (e[k] != kNone) orbit_acc(c[k], e[k], xv[k], acc, A.chi_tab);
+    }
+    const double sa = 1.0 / A.sqrtA[a];
+    double2 out = make_double2(acc.x * sa, acc.y * sa);
+    const double2 xa = x[a];
+    if (!tiny(xa)) {
+      const double dg = diag_value(S, u, d, S.cnt_uu[ru], S.cnt_dd[rd], S.wpl[ru]);
+      out.x = fma(dg, xa.x, out.x);
+      out.y = fma(dg, xa.y, out.y);
+    }
+    y[a] = out;
+  }
+}
+
 __global__ void scatter_kernel(const int64_t* __restrict__ full, int64_t n, int32_t* __restrict__ red) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t b = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; b < n; b += stride)
@@ -188,6 +291,11 @@ cudaError_t orbit_scatter_index(const int64_t* full, int64_t n, int32_t* red, cu
 
 cudaError_t orbit_apply(const OrbitApplyDev& A, const double2* x, double2* y, cudaStream_t st) {
   if (A.dk <= 0) return cudaSuccess;
+  if (A.path == 1 && A.xs != nullptr) {
+    prescale_kernel<<<grid_for(A.dk), 256, 0, st>>>(A.dk, A.sqrtA, x, A.xs);
+    apply_tables_kernel<<<grid_for(A.dk), 256, 0, st>>>(A, x, y);
+    return cudaGetLastError();
+  }
   apply_kernel<<<grid_for(A.dk), 256, 0, st>>>(A, x, y);
   return cudaGetLastError();
 }

@@ -53,6 +53,8 @@ struct OrbitApplyDev {
   const uint32_t* dhop_own;
   const uint32_t* dhop_oth;
   int n_dhops;
+  double2* xs;               // [dk] workspace: sqrt(|A_b|) x_b, zero where |x_b|^2 < 1e-28
+  int path;                  // 0: hop list per representative; 1: sector gather tables (default)
 };
 
 // red[full[b]] = b for b < n.

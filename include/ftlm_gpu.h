@@ -201,6 +201,9 @@ int ftlm_gpu_orbit_dim(const ftlm_orbit* o, long long* dim);
 /* Host copies of the reduced basis: packed representatives and |A(K)| (OrbitKRepEntry rep / abs_A). */
 int ftlm_gpu_orbit_entries(const ftlm_orbit* o, uint32_t* rep_packed, double* absA);
 int ftlm_gpu_orbit_apply(ftlm_orbit* o, const double* x_dev, double* y_dev, void* stream);
+/* 0: hop list scan per representative; 1 (default): the sector's gather tables, batched gathers.
+ * No reference counterpart (both compute apply_orbit_k_block). */
+int ftlm_gpu_orbit_set_apply_path(ftlm_orbit* o, int path);
 int ftlm_gpu_orbit_apply_host(ftlm_orbit* o, const double* x_host, double* y_host);
 /* ftlm_log_partition_complex on one block (seed_r = seed + r*100003). */
 int ftlm_gpu_orbit_ftlm(ftlm_orbit* o, const double* bts, int n_bt, int R, int M, unsigned seed, int start_mode,

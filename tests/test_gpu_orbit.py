@@ -65,9 +65,11 @@ def test_orbit_apply_matches_oracle(gpu, case):
         x = rng.standard_normal(o.dim) + 1j * rng.standard_normal(o.dim)
         x[rng.random(o.dim) < 0.05] = 0.0
         x[rng.random(o.dim) < 0.05] = 3e-15  # below the 1e-28 |x|^2 skip threshold
-        y = o.apply_host(x)
         yr = oo.apply(x)
-        assert np.abs(y - yr).max() <= RTOL_APPLY * np.abs(yr).max()
+        for path in (0, 1):
+            o.set_apply_path(path)
+            y = o.apply_host(x)
+            assert np.abs(y - yr).max() <= RTOL_APPLY * np.abs(yr).max(), path
 
 
 def test_orbit_apply_device_pointers(gpu):
