@@ -17,6 +17,7 @@ FTLM_ERR_CUDA = 2
 FTLM_ERR_NOMEM = 3
 FTLM_ERR_TIMEOUT = 4
 FTLM_ERR_UNSUPPORTED = 5
+FTLM_ERR_NUMERIC = 6
 FTLM_START_REFERENCE = 0
 FTLM_START_PHILOX = 1
 
@@ -86,6 +87,9 @@ SIGNATURES = {
     "ftlm_gpu_batched_ftlm_sector": [_vp, _vp, _i, _i, _i, C.c_uint, _vp, _vp],
     "ftlm_gpu_batched_sweep": [C.POINTER(FtlmParams), _i, _i, C.c_uint, _vp, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp],
     "ftlm_gpu_batched_release": [],
+    "ftlm_gpu_grad_sector": [_vp, _vp, _d, _i, _i, C.c_uint, _i, _i, _vp, _vp],
+    "ftlm_gpu_tridiag_eigvec": [_vp, _vp, _i, _vp, _vp],
+    "ftlm_gpu_duhamel_weights": [_vp, _vp, _i, _d, _vp, _vp, _vp],
     "ftlm_gpu_orbit_create": [_vp, _i, _i, C.POINTER(_vp)],
     "ftlm_gpu_orbit_destroy": [_vp],
     "ftlm_gpu_orbit_set_apply_path": [_vp, _i],

@@ -282,6 +282,19 @@ class Sector(_Handle):
         return lnz, en
 
 
+    def ftlm_grad(self, beta: float, n_random: int, lanczos_steps: int, seed: int, op_tp: Optional["Sector"] = None,
+                  method: str = "plain", start: str = "reference"):
+        """Sector ln Z estimate at inverse temperature beta and its derivatives with respect to
+        (U, V, t') with the start vectors held fixed, from a replay of the forward's chains
+        (method "plain" = ftlm(start=...), "batched" = batched_ftlm).  op_tp: the same sector built
+        with t=0, t'=1, U=V=0 (dH/dt'); without it the t' derivative is 0."""
+        lnz = C.c_double()
+        d = np.zeros(3)
+        call("ftlm_gpu_grad_sector", self._h, op_tp.handle if op_tp is not None else None, float(beta), n_random,
+             lanczos_steps, C.c_uint(seed & 0xFFFFFFFF), {"plain": 0, "batched": 1}[method], START_MODES[start],
+             C.byref(lnz), d.ctypes.data_as(C.c_void_p))
+        return lnz.value, d
+
     def orbit_block(self, kx: int, ky: int) -> "OrbitKBlock":
         return OrbitKBlock(self, kx, ky)
 

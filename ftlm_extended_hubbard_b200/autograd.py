@@ -1,0 +1,118 @@
+"""Differentiable grand-canonical FTLM: ln Z_GC(U, V, t', mu, beta) as a torch.autograd.Function.
+
+Forward: every (N_up, N_dn) sector's FTLM ln Z_s at beta (batched complex64 chains, or the plain
+complex128 chains with the reference's start vectors), combined as
+    ln Z_GC = log sum_s exp(ln Z_s + beta mu N_s)
+(the grand-canonical reduction of benchmarks/bench_ftlm_nmu_rect.cpp:186-219 at one (T, mu)).
+Only per-sector ln Z_s and energies are kept; no Krylov vector outlives the forward.
+
+Backward (the reference has no derivatives):
+    d/dmu   = beta <N>,
+    d/dbeta = <mu N - E>          (E_s: the FTLM energy of the same quadrature, exact derivative),
+    d/dtheta for theta in (U, V, t'): sum_s w_s d ln Z_s/dtheta, w_s = exp(ln Z_s + beta mu N_s - ln Z_GC),
+where d ln Z_s/dtheta re-runs the sector's chains from their seed on the GPU
+(Sector.ftlm_grad: Duhamel derivative in each chain's Krylov space, start vectors fixed).
+Sectors with w_s < 1e-13 are skipped (their term is below 1e-13 * beta * n_sites).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from .api import HubbardParams, Sector
+
+WEIGHT_CUTOFF = 1e-13
+
+
+@dataclass(frozen=True)
+class Lattice:
+    Lx: int
+    Ly: int
+    t: float = 1.0
+    phi_x: float = 0.0
+    phi_y: float = 0.0
+
+
+def _sector_lnz(lat: Lattice, U, V, tp, beta, nu, nd, R, M, seed, method, start):
+    s = Sector(HubbardParams(lat.Lx, lat.Ly, lat.t, tp, U, V, lat.phi_x, lat.phi_y), nu, nd)
+    if method == "batched":
+        lz, en = s.batched_ftlm(beta, R, M, seed)
+    else:
+        lz, en = s.ftlm(beta, R, M, seed, start=start)
+    return float(lz[0]), float(en[0])
+
+
+def sector_table(lat: Lattice, theta, R, M, seed, method="batched", start="reference"):
+    """ln Z_s, E_s, N_s for every sector at theta = (U, V, t', mu, beta)."""
+    U, V, tp, mu, beta = (float(v) for v in theta)
+    n = lat.Lx * lat.Ly
+    lnz, en, N = [], [], []
+    for nu in range(n + 1):
+        for nd in range(n + 1):
+            lz, e = _sector_lnz(lat, U, V, tp, beta, nu, nd, R, M, seed, method, start)
+            lnz.append(lz)
+            en.append(e)
+            N.append(nu + nd)
+    return np.array(lnz), np.array(en), np.array(N, dtype=np.float64)
+
+
+def _lse(x):
+    m = np.max(x)
+    return float(m + np.log(np.sum(np.exp(x - m))))
+
+
+def grand_canonical_logz_value(lat: Lattice, theta, R, M, seed, method="batched", start="reference") -> float:
+    lnz, _, N = sector_table(lat, theta, R, M, seed, method, start)
+    return _lse(lnz + float(theta[4]) * float(theta[3]) * N)
+
+
+class GrandCanonicalLogZ(torch.autograd.Function):
+    """theta: float64 tensor (U, V, t', mu, beta).  Returns the scalar ln Z_GC."""
+
+    @staticmethod
+    def forward(ctx, theta, lat: Lattice, R: int, M: int, seed: int, method: str = "batched",
+                start: str = "reference"):
+        th = theta.detach().cpu().double().numpy()
+        lnz, en, N = sector_table(lat, th, R, M, seed, method, start)
+        x = lnz + th[4] * th[3] * N
+        lnZ = _lse(x)
+        ctx.save_for_backward(theta)
+        ctx.cfg = (lat, R, M, seed, method, start)
+        ctx.table = (lnz, en, N, lnZ)
+        return theta.new_tensor(lnZ)
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        (theta,) = ctx.saved_tensors
+        lat, R, M, seed, method, start = ctx.cfg
+        lnz, en, N, lnZ = ctx.table
+        U, V, tp, mu, beta = (float(v) for v in theta.detach().cpu().double().numpy())
+        w = np.exp(lnz + beta * mu * N - lnZ)
+        d = np.zeros(3)
+        n = lat.Lx * lat.Ly
+        k = 0
+        for nu in range(n + 1):
+            for nd in range(n + 1):
+                ws = w[k]
+                k += 1
+                if not ws >= WEIGHT_CUTOFF:
+                    continue
+                p = HubbardParams(lat.Lx, lat.Ly, lat.t, tp, U, V, lat.phi_x, lat.phi_y)
+                s = Sector(p, nu, nd)
+                op = Sector(HubbardParams(lat.Lx, lat.Ly, 0.0, 1.0, 0.0, 0.0, lat.phi_x, lat.phi_y), nu, nd)
+                lz, g = s.ftlm_grad(beta, R, M, seed, op_tp=op, method=method, start=start)
+                if not abs(lz - lnz[k - 1]) <= 1e-9 * max(1.0, abs(lz)):
+                    raise RuntimeError(f"gradient replay of sector ({nu},{nd}) did not reproduce the forward "
+                                       f"ln Z ({lz} vs {lnz[k - 1]})")
+                d += ws * g
+        dmu = beta * float(np.sum(w * N))
+        dbeta = float(np.sum(w * (mu * N - en)))
+        grad = theta.new_tensor([d[0], d[1], d[2], dmu, dbeta])
+        return grad_out * grad, None, None, None, None, None, None
+
+
+def grand_canonical_logz(theta: torch.Tensor, lat: Lattice, R: int, M: int, seed: int, method: str = "batched",
+                         start: str = "reference") -> torch.Tensor:
+    return GrandCanonicalLogZ.apply(theta, lat, R, M, seed, method, start)

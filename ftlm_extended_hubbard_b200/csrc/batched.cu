@@ -460,4 +460,11 @@ cudaError_t bt_step(const DevSector& S, const float2* Wk, const float2* Wkm1, fl
   return cudaGetLastError();
 }
 
+cudaError_t bt_apply(const DevSector& S, const float2* X, float2* Y, const double* st_unit, double* partial,
+                     const int* zero_flag, cudaStream_t s) {
+  bt_rows_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(S, X, Y, st_unit, zero_flag);
+  bt_cols_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(S, X, Y, st_unit, partial, zero_flag);
+  return cudaGetLastError();
+}
+
 }  // namespace ftlm_b200

@@ -27,4 +27,9 @@ cudaError_t bt_start(float2* W, int64_t dim, unsigned seed, double* st, double* 
 cudaError_t bt_step(const DevSector& S, const float2* Wk, const float2* Wkm1, float2* Y, int k, double* st,
                     double* partial, double* alpha, double* beta, int* used, int* flags, cudaStream_t s);
 
+// Y = H X for one block vector, without Lanczos bookkeeping: st_unit holds kBtSin = 1 for every
+// chain, zero_flag points to an int 0 (no small-entry filter), partial receives unused dot sums.
+cudaError_t bt_apply(const DevSector& S, const float2* X, float2* Y, const double* st_unit, double* partial,
+                     const int* zero_flag, cudaStream_t s);
+
 }  // namespace ftlm_b200

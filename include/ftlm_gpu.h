@@ -38,6 +38,7 @@ extern "C" {
 #define FTLM_ERR_NOMEM 3       /* device or host allocation failed */
 #define FTLM_ERR_TIMEOUT 4     /* a bounded device-side wait ran out */
 #define FTLM_ERR_UNSUPPORTED 5 /* outside the sizes this build supports */
+#define FTLM_ERR_NUMERIC 6     /* a dense eigen-solver did not converge */
 
 /* Mirrors ftlm::HubbardParams (include/ftlm/hubbard_params.hpp:6-15). */
 typedef struct ftlm_params {
@@ -213,6 +214,26 @@ int ftlm_gpu_orbit_ftlm(ftlm_orbit* o, const double* bts, int n_bt, int R, int M
  * (may be NULL) receives the block dimensions. */
 int ftlm_gpu_orbit_sector_ftlm(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed,
                                int sector_index, int start_mode, double* lnz, double* energy, long long* dims_k);
+
+/* ---- parameter gradient of the sector FTLM estimate (no counterpart in the reference) ----
+ * Replays the chains of ftlm_gpu_ftlm_sector (method 0, start_mode as there) or of
+ * ftlm_gpu_batched_ftlm_sector (method 1; complex64 32-chain blocks, sectors with
+ * dim <= 2M on the complex128 Philox path as there) from their seed, keeps their Lanczos vectors
+ * on the device and returns
+ *   lnz      the sector ln Z estimate at inverse temperature bT (the forward call's value),
+ *   dlnz[3]  d lnZ/dU, d lnZ/dV, d lnZ/dt' of that estimate with the start vectors fixed: per
+ *            chain the Duhamel derivative -sum_il K_il <q_i|dH/dtheta|q_l> of e_1^T e^{-bT T} e_1.
+ * op_tp is a sector of the same (n_sites, N_up, N_dn) built with t = 0, t' = 1, U = V = 0 (the
+ * operator dH/dt'), or NULL (dlnz[2] = 0).  Device memory: M (M+1 for method 1) vectors of the
+ * sector, twice with op_tp; released by ftlm_gpu_batched_release. */
+int ftlm_gpu_grad_sector(ftlm_sector* s, ftlm_sector* op_tp, double bT, int R, int M, unsigned seed, int method,
+                         int start_mode, double* lnz, double* dlnz);
+/* Host-only dense helpers behind the gradient (no reference counterpart): eigen-decomposition of
+ * a symmetric tridiagonal (implicit QL; lam ascending, Z row-major with eigenvectors in columns),
+ * and the Duhamel weight matrix K (n x n) with g = e_1^T e^{-bT (T - lam_min)} e_1. */
+int ftlm_gpu_tridiag_eigvec(const double* alpha, const double* beta, int n, double* lam, double* Z);
+int ftlm_gpu_duhamel_weights(const double* alpha, const double* beta, int n, double bT, double* K, double* g,
+                             double* lam_min);
 
 #ifdef __cplusplus
 }
