@@ -89,6 +89,7 @@ SIGNATURES = {
     "ftlm_gpu_batched_release": [],
     "ftlm_gpu_grad_sector": [_vp, _vp, _d, _i, _i, C.c_uint, _i, _i, _vp, _vp],
     "ftlm_gpu_tridiag_eigvec": [_vp, _vp, _i, _vp, _vp],
+    "ftlm_gpu_tridiag_quadrature_exact": [_vp, _vp, _vp, _i, _i, _vp, _i, _vp, _vp],
     "ftlm_gpu_duhamel_weights": [_vp, _vp, _i, _d, _vp, _vp, _vp],
     "ftlm_gpu_orbit_create": [_vp, _i, _i, C.POINTER(_vp)],
     "ftlm_gpu_orbit_destroy": [_vp],

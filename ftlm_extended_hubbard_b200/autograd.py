@@ -1,7 +1,8 @@
 """Differentiable grand-canonical FTLM: ln Z_GC(U, V, t', mu, beta) as a torch.autograd.Function.
 
 Forward: every (N_up, N_dn) sector's FTLM ln Z_s at beta (batched complex64 chains, or the plain
-complex128 chains with the reference's start vectors), combined as
+complex128 chains with the reference's start vectors; the tridiagonal quadrature from a converged
+eigen-decomposition, which the gradient differentiates exactly), combined as
     ln Z_GC = log sum_s exp(ln Z_s + beta mu N_s)
 (the grand-canonical reduction of benchmarks/bench_ftlm_nmu_rect.cpp:186-219 at one (T, mu)).
 Only per-sector ln Z_s and energies are kept; no Krylov vector outlives the forward.
@@ -21,6 +22,9 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
+import ctypes as C
+
+from ._lib import call
 from .api import HubbardParams, Sector
 
 WEIGHT_CUTOFF = 1e-13
@@ -35,13 +39,37 @@ class Lattice:
     phi_y: float = 0.0
 
 
+def _chains(s: Sector, R, M, seed, method, start):
+    """alpha/beta [R][M] and steps used of the forward's chains (same seeds as ftlm/batched_ftlm)."""
+    if method == "batched" and s.dim() > 2 * M:
+        return s.batched_lanczos(R, M, seed)
+    st = "philox" if method == "batched" else start
+    A = np.zeros((R, M))
+    B = np.zeros((R, M))
+    used = np.zeros(R, np.int32)
+    for r in range(R):
+        a, b, u = s.lanczos(M, (seed + r * 100003) & 0xFFFFFFFF, start=st)
+        A[r, :a.size] = a
+        B[r, :b.size] = b
+        used[r] = u
+    return A, B, used
+
+
 def _sector_lnz(lat: Lattice, U, V, tp, beta, nu, nd, R, M, seed, method, start):
     s = Sector(HubbardParams(lat.Lx, lat.Ly, lat.t, tp, U, V, lat.phi_x, lat.phi_y), nu, nd)
-    if method == "batched":
-        lz, en = s.batched_ftlm(beta, R, M, seed)
-    else:
-        lz, en = s.ftlm(beta, R, M, seed, start=start)
-    return float(lz[0]), float(en[0])
+    A, B, used = _chains(s, R, M, seed, method, start)
+    bt = np.array([float(beta)])
+    lq = np.zeros((R, 1))
+    eq = np.zeros((R, 1))
+    call("ftlm_gpu_tridiag_quadrature_exact", _p(A), _p(B), _p(used), R, M, _p(bt), 1, _p(lq), _p(eq))
+    lnz = np.zeros(1)
+    en = np.zeros(1)
+    call("ftlm_gpu_ftlm_combine", _p(lq), _p(eq), _p(used), R, 1, float(np.log(s.dim())), _p(lnz), _p(en))
+    return float(lnz[0]), float(en[0])
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
 
 
 def sector_table(lat: Lattice, theta, R, M, seed, method="batched", start="reference"):

@@ -1247,6 +1247,45 @@ int ftlm_gpu_grad_sector(ftlm_sector* s, ftlm_sector* op_tp, double bT, int R, i
   return FTLM_OK;
 }
 
+// Per-chain log quadrature and energy ratio with a converged eigen-decomposition (host QL), the
+// quadrature the gradient differentiates; same layout as ftlm_gpu_tridiag_quadrature.
+int ftlm_gpu_tridiag_quadrature_exact(const double* alpha, const double* beta, const int* n, int nc, int ld,
+                                      const double* bts, int n_bt, double* logq, double* energy) {
+  if (nc < 0 || ld <= 0 || n_bt < 0 || !alpha || !beta || !n || (n_bt > 0 && (!bts || !logq || !energy)))
+    return fail(FTLM_ERR_INVALID, "bad arguments");
+  std::vector<double> lam, Z;
+  for (int c = 0; c < nc; ++c) {
+    const int nn = n[c];
+    if (nn > ld) return fail(FTLM_ERR_INVALID, "chain length exceeds ld");
+    double* lq = logq + static_cast<size_t>(c) * n_bt;
+    double* eq = energy + static_cast<size_t>(c) * n_bt;
+    if (nn <= 0) {
+      for (int b = 0; b < n_bt; ++b) {
+        lq[b] = -std::numeric_limits<double>::infinity();
+        eq[b] = 0.0;
+      }
+      continue;
+    }
+    lam.assign(static_cast<size_t>(nn), 0.0);
+    Z.assign(static_cast<size_t>(nn) * nn, 0.0);
+    const std::string err = tridiag_eigvec(nn, alpha + static_cast<size_t>(c) * ld, beta + static_cast<size_t>(c) * ld,
+                                           lam.data(), Z.data());
+    if (!err.empty()) return fail(FTLM_ERR_NUMERIC, err);
+    for (int b = 0; b < n_bt; ++b) {
+      const double bT = bts[b];
+      double z = 0.0, ze = 0.0;
+      for (int j = 0; j < nn; ++j) {
+        const double w = Z[static_cast<size_t>(j)] * Z[static_cast<size_t>(j)] * std::exp(-bT * (lam[static_cast<size_t>(j)] - lam[0]));
+        z += w;
+        ze += w * lam[static_cast<size_t>(j)];
+      }
+      lq[b] = -bT * lam[0] + std::log(z);
+      eq[b] = ze / z;
+    }
+  }
+  return FTLM_OK;
+}
+
 // Host-only helper exposed for tests: eigenvalues/eigenvectors of a symmetric tridiagonal.
 int ftlm_gpu_tridiag_eigvec(const double* alpha, const double* beta, int n, double* lam, double* Z) {
   if (n < 0 || (n > 0 && (!alpha || !lam || !Z || (n > 1 && !beta)))) return fail(FTLM_ERR_INVALID, "bad arguments");

@@ -128,14 +128,19 @@ cudaError_t launch(const DevSector& S, const T* W, const T* AW, int64_t vstride,
 
 }  // namespace
 
+// Widest block whose slice of the n vectors fits in shared memory.
 cudaError_t grad_moments_c64(const DevSector& S, const float2* W, const float2* AW, int64_t vstride, const double* Kp,
                              int n, int ld, double* partial, int* grid, cudaStream_t st) {
-  return launch<float2, 32, 256>(S, W, AW, vstride, Kp, n, ld, partial, grid, st);
+  cudaError_t e = launch<float2, 32, 256>(S, W, AW, vstride, Kp, n, ld, partial, grid, st);
+  if (e == cudaErrorInvalidValue) e = launch<float2, 32, 128>(S, W, AW, vstride, Kp, n, ld, partial, grid, st);
+  return e;
 }
 
 cudaError_t grad_moments_c128(const DevSector& S, const double2* W, const double2* AW, int64_t vstride,
                               const double* Kp, int n, int ld, double* partial, int* grid, cudaStream_t st) {
-  return launch<double2, 1, 128>(S, W, AW, vstride, Kp, n, ld, partial, grid, st);
+  cudaError_t e = launch<double2, 1, 128>(S, W, AW, vstride, Kp, n, ld, partial, grid, st);
+  if (e == cudaErrorInvalidValue) e = launch<double2, 1, 64>(S, W, AW, vstride, Kp, n, ld, partial, grid, st);
+  return e;
 }
 
 }  // namespace ftlm_b200

@@ -232,6 +232,12 @@ int ftlm_gpu_grad_sector(ftlm_sector* s, ftlm_sector* op_tp, double bT, int R, i
  * a symmetric tridiagonal (implicit QL; lam ascending, Z row-major with eigenvectors in columns),
  * and the Duhamel weight matrix K (n x n) with g = e_1^T e^{-bT (T - lam_min)} e_1. */
 int ftlm_gpu_tridiag_eigvec(const double* alpha, const double* beta, int n, double* lam, double* Z);
+/* Per-chain log e_1^T e^{-bT T} e_1 and energy ratio from that converged decomposition (layout of
+ * ftlm_gpu_tridiag_quadrature).  The reference's Jacobi stops after max(3000, 120 n) rotations; for
+ * n ~ 80 at low temperature the two differ by up to ~1e-7 in a chain's log quadrature, and the
+ * differentiable path uses this one in forward and backward. */
+int ftlm_gpu_tridiag_quadrature_exact(const double* alpha, const double* beta, const int* n, int nc, int ld,
+                                      const double* bts, int n_bt, double* logq, double* energy);
 int ftlm_gpu_duhamel_weights(const double* alpha, const double* beta, int n, double bT, double* K, double* g,
                              double* lam_min);
 
