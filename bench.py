@@ -45,9 +45,13 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--sector", type=int, nargs=2, default=None, metavar=("NU", "ND"),
                     help="profile a smaller 4x4 sector instead (for ncu captures); not a bench line")
-    ap.add_argument("--workload", default="hv", choices=["hv", "batched"],
-                    help="hv: the H·v benchmark; batched: 32-chain complex64 Lanczos steps on one sector "
-                         "(profiling aid, prints chain-steps/s)")
+    ap.add_argument("--workload", default="hv", choices=["hv", "batched", "sweep-model", "orbit", "grad"],
+                    help="hv: the H·v benchmark (the bench line).  Measurement aids (one JSON line each, not "
+                         "bench lines): batched = 32-chain complex64 Lanczos steps on one sector; sweep-model = "
+                         "per-sector step cost of the plain and batched paths over the full 4x4 sweep (R=32, "
+                         "M=100) and the modelled sweep times; orbit = H_K·v of one momentum block; grad = "
+                         "forward and backward of the differentiable 4x3 ln Z_GC (R=32, M=80)")
+    ap.add_argument("--k", type=int, nargs=2, default=(1, 2), metavar=("KX", "KY"), help="orbit workload momentum")
     return ap.parse_args()
 
 
@@ -382,12 +386,104 @@ def run_batched(args):
     return 0
 
 
+def run_sweep_model(args):
+    """Per-sector Lanczos step cost of both paths on every 4x4 sector class (dims equal under
+    N -> 16-N and spin exchange), combined into the time of a full R=32, M=100 sweep."""
+    import torch
+    import ftlm_extended_hubbard_b200 as F
+    n, R, M, S = 16, 32, 100, max(1, args.steps)
+    classes = {}
+    for nu in range(n + 1):
+        for nd in range(n + 1):
+            a, b = min(nu, n - nu), min(nd, n - nd)
+            classes.setdefault((min(a, b), max(a, b)), []).append((nu, nd))
+    recs, t_plain, t_batched = [], 0.0, 0.0
+    for (a, b), members in sorted(classes.items()):
+        s = F.Sector(F.HubbardParams(**PARAMS), a, b)
+        s.lanczos(1, 1, start="philox")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.lanczos(S, 5, start="philox")
+        tp = (time.perf_counter() - t0) / S
+        rec = {"nu": a, "nd": b, "dim": s.dim(), "sectors": len(members), "plain_chain_step_ms": 1e3 * tp}
+        plain = R * M * tp
+        bat = plain
+        if s.dim() > 2 * M:
+            s.batched_lanczos(32, 2, 1)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s.batched_lanczos(32, S, 1)
+            tb = (time.perf_counter() - t0) / S
+            rec["batched_block_step_ms"] = 1e3 * tb
+            bat = M * tb * ((R + 31) // 32)
+        t_plain += len(members) * plain
+        t_batched += len(members) * bat
+        recs.append(rec)
+        s.close()
+        F.batched_release()
+    print(json.dumps({"workload": "4x4 sweep model, R=32, M=100, complex128 plain vs complex64 batched",
+                      "plain_sweep_s": t_plain, "batched_sweep_s": t_batched, "ratio": t_plain / t_batched,
+                      "steps_timed_per_sector": S, "sectors": recs}))
+    return 0
+
+
+def run_orbit(args):
+    """H_K·v of one translation-orbit block (default 4x4 (8,8), K=(1,2), U=6, V=0.5, phi=0)."""
+    import torch
+    import ftlm_extended_hubbard_b200 as F
+    nu, nd = args.sector if args.sector else (NU, ND)
+    p = F.HubbardParams(4, 4, 1.0, -0.25, 6.0, 0.5, 0.0, 0.0)
+    s = F.Sector(p, nu, nd)
+    t0 = time.perf_counter()
+    o = s.orbit_block(*args.k)
+    build = time.perf_counter() - t0
+    x = torch.randn(o.dim, dtype=torch.complex128, device="cuda")
+    y = torch.empty_like(x)
+    for _ in range(max(1, args.warmup)):
+        o.apply(x, y)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        o.apply(x, y)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    print(json.dumps({"workload": f"orbit H_K v, 4x4 ({nu},{nd}) K={tuple(args.k)}", "block_dim": o.dim,
+                      "ms_per_apply": ms, "reps_per_s": o.dim / ms * 1e3, "block_build_s": build}))
+    o.close()
+    return 0
+
+
+def run_grad(args):
+    """Forward + backward of ln Z_GC(U, V, t', mu, beta) on the 4x3 lattice (169 sectors, R=32, M=80,
+    batched complex64 chains) at theta = (4, 1, -0.2, 2, 5)."""
+    import numpy as np
+    import torch
+    from ftlm_extended_hubbard_b200 import autograd as AG
+    theta = torch.tensor([4.0, 1.0, -0.2, 2.0, 5.0], dtype=torch.float64, requires_grad=True)
+    t0 = time.perf_counter()
+    lnz = AG.grand_canonical_logz(theta, AG.Lattice(4, 3), 32, 80, 7, method="batched")
+    t1 = time.perf_counter()
+    lnz.backward()
+    t2 = time.perf_counter()
+    print(json.dumps({"workload": "d lnZ_GC / d(U, V, t', mu, beta), 4x3, R=32, M=80", "lnZ": lnz.item(),
+                      "grad": np.asarray(theta.grad).tolist(), "forward_s": t1 - t0, "backward_s": t2 - t1}))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batched":
         return run_batched(args)
+    if args.workload == "sweep-model":
+        return run_sweep_model(args)
+    if args.workload == "orbit":
+        return run_orbit(args)
+    if args.workload == "grad":
+        return run_grad(args)
     return run_ours(args)
 
 
