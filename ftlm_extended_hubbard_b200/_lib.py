@@ -92,6 +92,9 @@ SIGNATURES = {
     "ftlm_gpu_tridiag_quadrature_exact": [_vp, _vp, _vp, _i, _i, _vp, _i, _vp, _vp],
     "ftlm_gpu_duhamel_weights": [_vp, _vp, _i, _d, _vp, _vp, _vp],
     "ftlm_gpu_orbit_create": [_vp, _i, _i, C.POINTER(_vp)],
+    "ftlm_gpu_orbit_create_ex": [_vp, _i, _i, _d, C.POINTER(_vp)],
+    "ftlm_gpu_sector_set_lattice": [_vp, _i, _i],
+    "ftlm_gpu_orbit_entries_ex": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "ftlm_gpu_orbit_destroy": [_vp],
     "ftlm_gpu_orbit_set_apply_path": [_vp, _i],
     "ftlm_gpu_orbit_dim": [_vp, C.POINTER(_ll)],

@@ -2,6 +2,7 @@
 // libftlm_gpu.so.  Host orchestration only: every H·v, Lanczos step and quadrature runs in the
 // library's CUDA kernels.  Errors become the reference's exceptions (std::invalid_argument for
 // bad sectors, std::out_of_range for FockBasis indices, std::runtime_error otherwise).
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstring>
@@ -20,6 +21,7 @@
 #include "ftlm/lanczos.hpp"
 #include "ftlm/lanczos_engine.hpp"
 #include "ftlm/lattice.hpp"
+#include "ftlm/symmetry/orbit_k_block_basis.hpp"
 #include "ftlm/version.hpp"
 #include "ftlm_gpu.h"
 
@@ -265,5 +267,176 @@ double ftlm_log_partition_real(int dim, const std::function<void(const double*, 
     return y[0];
   });
 }
+
+// ---- translation-orbit momentum blocks (include/ftlm/symmetry/orbit_k_block_basis.hpp) ---------
+namespace symmetry {
+
+namespace {
+
+// Site (x, y) = y*lx + x goes to ((y+dy) mod ly)*lx + (x+dx) mod lx.
+int shift_site(int site, int lx, int ly, int dx, int dy) {
+  return ((site / lx + dy) % ly) * lx + (site % lx + dx) % lx;
+}
+
+std::uint16_t shift_bits(std::uint16_t m, int lx, int ly, int dx, int dy) {
+  std::uint32_t out = 0;
+  for (int site = 0; site < lx * ly; ++site)
+    if ((m >> site) & 1u) out |= 1u << shift_site(site, lx, ly, dx, dy);
+  return static_cast<std::uint16_t>(out);
+}
+
+// (-1)^(inversions of the occupied modes 2*site+spin, in site order, after the translation).
+double shift_sign(RawState s, int lx, int ly, int dx, int dy) {
+  int modes[32];
+  int n = 0;
+  for (int site = 0; site < lx * ly; ++site) {
+    const int t = shift_site(site, lx, ly, dx, dy);
+    if ((s.up >> site) & 1u) modes[n++] = 2 * t;
+    if ((s.dn >> site) & 1u) modes[n++] = 2 * t + 1;
+  }
+  int inv = 0;
+  for (int i = 0; i < n; ++i)
+    for (int j = i + 1; j < n; ++j) inv += modes[i] > modes[j] ? 1 : 0;
+  return (inv & 1) ? -1.0 : 1.0;
+}
+
+RawState canonical(RawState s, int lx, int ly) {
+  std::uint32_t best = pack_raw_state(s);
+  for (int dy = 0; dy < ly; ++dy)
+    for (int dx = 0; dx < lx; ++dx) {
+      const RawState t{shift_bits(s.up, lx, ly, dx, dy), shift_bits(s.dn, lx, ly, dx, dy)};
+      best = std::min(best, pack_raw_state(t));
+    }
+  return unpack_raw_state(best);
+}
+
+ftlm_sector* bare_sector(const FockBasis& fb, int lx, int ly) {
+  ftlm_sector* s = nullptr;
+  check(ftlm_gpu_sector_create_hops(fb.n_sites(), fb.n_up(), fb.n_down(), 0.0, 0.0, nullptr, 0, nullptr, 0, &s));
+  const int rc = ftlm_gpu_sector_set_lattice(s, lx, ly);
+  if (rc != FTLM_OK) {
+    const std::string msg = ftlm_gpu_last_error();
+    ftlm_gpu_sector_destroy(s);
+    throw std::invalid_argument(msg);
+  }
+  return s;
+}
+
+// Device sector + orbit block per (operator, K, tolerance); both destroyed together on eviction.
+struct OrbitSlot {
+  ftlm_sector* s = nullptr;
+  ftlm_orbit* o = nullptr;
+};
+std::mutex g_orbit_mu;
+std::map<std::string, OrbitSlot> g_orbits;
+
+}  // namespace
+
+bool OrbitKBlockBasis::build(const FockBasis& fb, MomentumSector Ksec, double survive_tol) {
+  entries_.clear();
+  rep_pack_to_row_.clear();
+  survive_tol_ = survive_tol;
+  K = Ksec;
+  lx = K.lx;
+  ly = K.ly;
+  if (fb.n_sites() > 16)
+    throw std::invalid_argument("OrbitKBlockBasis::build: n_sites must be <= 16 (RawState bit width)");
+  ftlm_sector* s = bare_sector(fb, lx, ly);
+  ftlm_orbit* o = nullptr;
+  int rc = ftlm_gpu_orbit_create_ex(s, K.kx, K.ky, survive_tol, &o);
+  if (rc != FTLM_OK) {
+    ftlm_gpu_sector_destroy(s);
+    check(rc);
+  }
+  long long d = 0;
+  ftlm_gpu_orbit_dim(o, &d);
+  std::vector<std::uint32_t> rep(static_cast<size_t>(d));
+  std::vector<double> A(2 * static_cast<size_t>(d)), absA(static_cast<size_t>(d));
+  std::vector<int> osz(static_cast<size_t>(d)), ssz(static_cast<size_t>(d));
+  std::vector<long long> oidx(static_cast<size_t>(d));
+  rc = ftlm_gpu_orbit_entries_ex(o, rep.data(), A.data(), absA.data(), osz.data(), ssz.data(), oidx.data());
+  ftlm_gpu_orbit_destroy(o);
+  ftlm_gpu_sector_destroy(s);
+  check(rc);
+  entries_.resize(static_cast<size_t>(d));
+  for (size_t i = 0; i < entries_.size(); ++i) {
+    OrbitKRepEntry& e = entries_[i];
+    e.rep = unpack_raw_state(rep[i]);
+    e.orbit_index = static_cast<std::size_t>(oidx[i]);
+    e.orbit_size = static_cast<std::uint16_t>(osz[i]);
+    e.stabilizer_size = static_cast<std::uint16_t>(ssz[i]);
+    e.A_k = {A[2 * i], A[2 * i + 1]};
+    e.abs_A = absA[i];
+    rep_pack_to_row_[rep[i]] = i;
+  }
+  return true;
+}
+
+int OrbitKBlockBasis::reduced_index_of_rep(RawState rep) const {
+  const auto it = rep_pack_to_row_.find(pack_raw_state(rep));
+  return it == rep_pack_to_row_.end() ? -1 : static_cast<int>(it->second);
+}
+
+bool OrbitKBlockBasis::map_raw_to_rep(RawState s, int* reduced_index, int* dx, int* dy, double* eta) const {
+  if (!reduced_index || !dx || !dy || !eta) return false;
+  const RawState rep = canonical(s, lx, ly);
+  const auto it = rep_pack_to_row_.find(pack_raw_state(rep));
+  if (it == rep_pack_to_row_.end()) return false;
+  for (int tdx = 0; tdx < lx; ++tdx)
+    for (int tdy = 0; tdy < ly; ++tdy) {
+      if (shift_bits(rep.up, lx, ly, tdx, tdy) != s.up || shift_bits(rep.dn, lx, ly, tdx, tdy) != s.dn) continue;
+      *reduced_index = static_cast<int>(it->second);
+      *dx = tdx;
+      *dy = tdy;
+      *eta = shift_sign(rep, lx, ly, tdx, tdy);
+      return true;
+    }
+  return false;
+}
+
+void apply_orbit_k_block(const HubbardParams& p, const FockBasis& fb, const OrbitKBlockBasis& basis,
+                         const std::vector<SpinfulHopping>& hoppings, const std::vector<NearestPair>& nn_pairs,
+                         const std::complex<double>* x, std::complex<double>* y) {
+  const int dk = basis.dim();
+  if (dk <= 0) return;
+  std::string k = key_of(fb, p, hoppings, nn_pairs);
+  const int kk[4] = {basis.lx, basis.ly, basis.K.kx, basis.K.ky};
+  const double tol = basis.survive_tol();
+  k.append(reinterpret_cast<const char*>(kk), sizeof(kk));
+  k.append(reinterpret_cast<const char*>(&tol), sizeof(tol));
+  std::lock_guard<std::mutex> lock(g_orbit_mu);
+  auto it = g_orbits.find(k);
+  if (it == g_orbits.end()) {
+    if (g_orbits.size() >= 4) {
+      for (auto& kv : g_orbits) {
+        ftlm_gpu_orbit_destroy(kv.second.o);
+        ftlm_gpu_sector_destroy(kv.second.s);
+      }
+      g_orbits.clear();
+    }
+    std::vector<ftlm_hop> hv(hoppings.size());
+    for (size_t i = 0; i < hoppings.size(); ++i)
+      hv[i] = ftlm_hop{hoppings[i].from, hoppings[i].to, hoppings[i].spin, hoppings[i].coeff.real(),
+                       hoppings[i].coeff.imag()};
+    std::vector<ftlm_pair> pv(nn_pairs.size());
+    for (size_t i = 0; i < nn_pairs.size(); ++i) pv[i] = ftlm_pair{nn_pairs[i].i, nn_pairs[i].j};
+    OrbitSlot slot;
+    check(ftlm_gpu_sector_create_hops(fb.n_sites(), fb.n_up(), fb.n_down(), p.U, p.V, hv.data(),
+                                      static_cast<int>(hv.size()), pv.data(), static_cast<int>(pv.size()), &slot.s));
+    int rc = ftlm_gpu_sector_set_lattice(slot.s, basis.lx, basis.ly);
+    if (rc == FTLM_OK) rc = ftlm_gpu_orbit_create_ex(slot.s, basis.K.kx, basis.K.ky, tol, &slot.o);
+    if (rc != FTLM_OK) {
+      ftlm_gpu_sector_destroy(slot.s);
+      check(rc);
+    }
+    it = g_orbits.emplace(k, slot).first;
+  }
+  long long d = 0;
+  check(ftlm_gpu_orbit_dim(it->second.o, &d));
+  if (d != dk) throw std::invalid_argument("apply_orbit_k_block: basis does not belong to this sector");
+  check(ftlm_gpu_orbit_apply_host(it->second.o, reinterpret_cast<const double*>(x), reinterpret_cast<double*>(y)));
+}
+
+}  // namespace symmetry
 
 }  // namespace ftlm

@@ -1327,6 +1327,9 @@ struct ftlm_orbit {
   int64_t dk = 0;
   std::vector<uint32_t> reps;  // surviving representatives (ascending packed)
   std::vector<double> absA;
+  std::vector<double> Ak;         // A(K), 2 per representative
+  std::vector<int> stab;          // stabiliser size
+  std::vector<int64_t> orbit_idx; // index among all representatives of the sector (ascending packed)
   DevBuf reps_dev, sqrtA, table, chi, xs;
   OrbitApplyDev app{};
   LanczosWs ws;
@@ -1463,6 +1466,20 @@ int orbit_apply_dev(ftlm_orbit* o, const double2* x, double2* y, cudaStream_t st
 extern "C" {
 
 int ftlm_gpu_orbit_create(ftlm_sector* s, int kx, int ky, ftlm_orbit** out) {
+  return ftlm_gpu_orbit_create_ex(s, kx, ky, 1e-12, out);
+}
+
+int ftlm_gpu_sector_set_lattice(ftlm_sector* s, int Lx, int Ly) {
+  if (!s || Lx <= 0 || Ly <= 0 || Lx * Ly != s->plan.n)
+    return fail(FTLM_ERR_INVALID, "lattice Lx*Ly must equal the sector's number of sites");
+  if (s->Lx == Lx && s->Ly == Ly) return FTLM_OK;
+  s->Lx = Lx;
+  s->Ly = Ly;
+  s->orbit_data.reset();
+  return FTLM_OK;
+}
+
+int ftlm_gpu_orbit_create_ex(ftlm_sector* s, int kx, int ky, double survive_tol, ftlm_orbit** out) {
   int rc = need_device(s);
   if (rc) return rc;
   if (!out) return fail(FTLM_ERR_INVALID, "null output");
@@ -1488,18 +1505,28 @@ int ftlm_gpu_orbit_create(ftlm_sector* s, int kx, int ky, ftlm_orbit** out) {
     }
   CU_TRY(upload_to(o->chi, chi));
   const int64_t nreps = static_cast<int64_t>(D.reps_packed.size());
-  DevBuf absA;
+  DevBuf absA, Adev, sdev;
   CU_TRY(absA.alloc(std::max<int64_t>(nreps, 1) * sizeof(double)));
-  CU_TRY(orbit_absA(D.dev, D.reps_dev.as<uint32_t>(), nreps, o->chi.as<double2>(), absA.as<double>(), s->stream));
-  std::vector<double> aa(static_cast<size_t>(nreps));
+  CU_TRY(Adev.alloc(std::max<int64_t>(nreps, 1) * sizeof(double2)));
+  CU_TRY(sdev.alloc(std::max<int64_t>(nreps, 1) * sizeof(int)));
+  CU_TRY(orbit_absA(D.dev, D.reps_dev.as<uint32_t>(), nreps, o->chi.as<double2>(), absA.as<double>(),
+                    Adev.as<double2>(), sdev.as<int>(), s->stream));
+  std::vector<double> aa(static_cast<size_t>(nreps)), AA(static_cast<size_t>(nreps) * 2);
+  std::vector<int> ss(static_cast<size_t>(nreps));
   CU_TRY(cudaMemcpyAsync(aa.data(), absA.p, aa.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CU_TRY(cudaMemcpyAsync(AA.data(), Adev.p, AA.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CU_TRY(cudaMemcpyAsync(ss.data(), sdev.p, ss.size() * sizeof(int), cudaMemcpyDeviceToHost, s->stream));
   CU_TRY(cudaStreamSynchronize(s->stream));
   std::vector<int64_t> full;
   std::vector<double> sq;
   for (int64_t b = 0; b < nreps; ++b) {
-    if (aa[static_cast<size_t>(b)] <= 1e-12) continue;  // survive_tol (orbit_k_block_basis.hpp:53)
+    if (aa[static_cast<size_t>(b)] <= survive_tol) continue;  // survive_tol (orbit_k_block_basis.hpp:53)
     o->reps.push_back(D.reps_packed[static_cast<size_t>(b)]);
     o->absA.push_back(aa[static_cast<size_t>(b)]);
+    o->Ak.push_back(AA[2 * static_cast<size_t>(b)]);
+    o->Ak.push_back(AA[2 * static_cast<size_t>(b) + 1]);
+    o->stab.push_back(ss[static_cast<size_t>(b)]);
+    o->orbit_idx.push_back(b);
     full.push_back(D.reps_full[static_cast<size_t>(b)]);
     sq.push_back(std::sqrt(aa[static_cast<size_t>(b)]));
   }
@@ -1566,6 +1593,24 @@ int ftlm_gpu_orbit_entries(const ftlm_orbit* o, uint32_t* rep_packed, double* ab
   if (!o) return fail(FTLM_ERR_INVALID, "null orbit");
   if (rep_packed) std::copy(o->reps.begin(), o->reps.end(), rep_packed);
   if (absA) std::copy(o->absA.begin(), o->absA.end(), absA);
+  return FTLM_OK;
+}
+
+int ftlm_gpu_orbit_entries_ex(const ftlm_orbit* o, uint32_t* rep_packed, double* A, double* absA, int* orbit_size,
+                              int* stabilizer_size, long long* orbit_index) {
+  if (!o) return fail(FTLM_ERR_INVALID, "null orbit");
+  const int G = o->data->G;
+  for (size_t i = 0; i < o->reps.size(); ++i) {
+    if (rep_packed) rep_packed[i] = o->reps[i];
+    if (A) {
+      A[2 * i] = o->Ak[2 * i];
+      A[2 * i + 1] = o->Ak[2 * i + 1];
+    }
+    if (absA) absA[i] = o->absA[i];
+    if (stabilizer_size) stabilizer_size[i] = o->stab[i];
+    if (orbit_size) orbit_size[i] = o->stab[i] > 0 ? G / o->stab[i] : 0;
+    if (orbit_index) orbit_index[i] = o->orbit_idx[i];
+  }
   return FTLM_OK;
 }
 

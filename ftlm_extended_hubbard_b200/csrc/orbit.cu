@@ -62,18 +62,23 @@ __global__ void canon_kernel(OrbitDev O, int32_t* __restrict__ rep_full, uint8_t
 }
 
 __global__ void absA_kernel(OrbitDev O, const uint32_t* __restrict__ reps, int64_t nreps,
-                            const double2* __restrict__ chi_tab, double* __restrict__ absA) {
+                            const double2* __restrict__ chi_tab, double* __restrict__ absA, double2* __restrict__ Aout,
+                            int* __restrict__ stab) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t b = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; b < nreps; b += stride) {
     const uint32_t u = reps[b] >> 16, d = reps[b] & 0xFFFFu;
     double ar = 0.0, ai = 0.0;
+    int ns = 0;
     for (int R = 0; R < O.G; ++R) {  // dy outer, dx inner: R = dy * Lx + dx ascending
       if (translate(O, R, u) != u || translate(O, R, d) != d) continue;
+      ++ns;
       const double eta = translation_sign(O, R, u, d) ? -1.0 : 1.0;
       ar += eta * chi_tab[R].x;
       ai += eta * chi_tab[R].y;
     }
     absA[b] = hypot(ar, ai);
+    if (Aout) Aout[b] = make_double2(ar, ai);
+    if (stab) stab[b] = ns;
   }
 }
 
@@ -271,9 +276,9 @@ cudaError_t orbit_canon(const OrbitDev& O, int32_t* rep_full, uint8_t* reta, cud
 }
 
 cudaError_t orbit_absA(const OrbitDev& O, const uint32_t* reps, int64_t nreps, const double2* chi_tab, double* absA,
-                       cudaStream_t st) {
+                       double2* A, int* stab, cudaStream_t st) {
   if (nreps <= 0) return cudaSuccess;
-  absA_kernel<<<grid_for(nreps), 256, 0, st>>>(O, reps, nreps, chi_tab, absA);
+  absA_kernel<<<grid_for(nreps), 256, 0, st>>>(O, reps, nreps, chi_tab, absA, A, stab);
   return cudaGetLastError();
 }
 

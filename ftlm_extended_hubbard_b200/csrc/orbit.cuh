@@ -26,9 +26,10 @@ struct OrbitDev {
 // Per full state: full index of its canonical representative, and (R | eta<<4) with
 // T_R rep = state (first R in the reference's search order), eta = fermionic sign of T_R on rep.
 cudaError_t orbit_canon(const OrbitDev& O, int32_t* rep_full, uint8_t* reta, cudaStream_t st);
-// |A(K)| per representative: A = sum over stabiliser S of eta(rep,S) chi*(S) (chi* from chi_tab).
+// |A(K)| per representative: A = sum over stabiliser S of eta(rep,S) chi*(S) (chi* from chi_tab);
+// optionally A itself and the stabiliser size (A, stab may be null).
 cudaError_t orbit_absA(const OrbitDev& O, const uint32_t* reps_packed, int64_t nreps, const double2* chi_tab,
-                       double* absA, cudaStream_t st);
+                       double* absA, double2* A, int* stab, cudaStream_t st);
 // table[state] = beta | R<<24 | eta<<28 (beta = reduced index of its orbit at K) or 0xFFFFFFFF.
 cudaError_t orbit_table(const OrbitDev& O, const int32_t* rep_full, const uint8_t* reta, const int32_t* red_of_full,
                         uint32_t* table, cudaStream_t st);

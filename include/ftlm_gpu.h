@@ -197,10 +197,21 @@ int ftlm_gpu_batched_release(void);
  * Apply: apply_orbit_k_block (src/orbit_k_block_basis.cpp:151-220) on reduced complex128 vectors. */
 typedef struct ftlm_orbit ftlm_orbit;
 int ftlm_gpu_orbit_create(ftlm_sector* s, int kx, int ky, ftlm_orbit** out);
+/* Same with the survival threshold of OrbitKBlockBasis::build(fb, K, survive_tol)
+ * (include/ftlm/symmetry/orbit_k_block_basis.hpp:53, default 1e-12). */
+int ftlm_gpu_orbit_create_ex(ftlm_sector* s, int kx, int ky, double survive_tol, ftlm_orbit** out);
+/* Tag a sector built from hop lists with its Lx x Ly rectangle (site = y*Lx + x), so that orbit
+ * blocks can be built on it (MomentumSector K carries lx, ly in the reference). */
+int ftlm_gpu_sector_set_lattice(ftlm_sector* s, int Lx, int Ly);
 int ftlm_gpu_orbit_destroy(ftlm_orbit* o);
 int ftlm_gpu_orbit_dim(const ftlm_orbit* o, long long* dim);
 /* Host copies of the reduced basis: packed representatives and |A(K)| (OrbitKRepEntry rep / abs_A). */
 int ftlm_gpu_orbit_entries(const ftlm_orbit* o, uint32_t* rep_packed, double* absA);
+/* All OrbitKRepEntry fields (orbit_k_block_basis.hpp:35-42): rep, A_k (2 doubles each), abs_A,
+ * orbit_size, stabilizer_size, orbit_index (index into the sector's orbit list, which the reference
+ * builds in ascending packed order of the representatives).  Any pointer may be NULL. */
+int ftlm_gpu_orbit_entries_ex(const ftlm_orbit* o, uint32_t* rep_packed, double* A, double* absA, int* orbit_size,
+                              int* stabilizer_size, long long* orbit_index);
 int ftlm_gpu_orbit_apply(ftlm_orbit* o, const double* x_dev, double* y_dev, void* stream);
 /* 0: hop list scan per representative; 1 (default): the sector's gather tables, batched gathers.
  * No reference counterpart (both compute apply_orbit_k_block). */

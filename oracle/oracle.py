@@ -27,6 +27,9 @@ def build(ref: bool = True) -> None:
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
     if ref and os.path.isdir(os.path.join(REFERENCE_SRC, "src")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REFERENCE_SRC}"], check=True)
+        # the reference's own test/driver programs compiled against the C++ drop-in (needs libftlm_dropin.so)
+        if os.path.exists(os.path.join(os.path.dirname(HERE), "ftlm_extended_hubbard_b200", "libftlm_dropin.so")):
+            subprocess.run(["make", "-s", "-C", HERE, "dropin", f"REF={REFERENCE_SRC}"], check=True)
 
 
 def P(a: np.ndarray) -> C.c_void_p:
