@@ -45,12 +45,14 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--sector", type=int, nargs=2, default=None, metavar=("NU", "ND"),
                     help="profile a smaller 4x4 sector instead (for ncu captures); not a bench line")
-    ap.add_argument("--workload", default="hv", choices=["hv", "batched", "sweep-model", "orbit", "grad"],
+    ap.add_argument("--workload", default="hv", choices=["hv", "batched", "sweep-model", "orbit", "grad", "kresolved"],
                     help="hv: the H·v benchmark (the bench line).  Measurement aids (one JSON line each, not "
                          "bench lines): batched = 32-chain complex64 Lanczos steps on one sector; sweep-model = "
                          "per-sector step cost of the plain and batched paths over the full 4x4 sweep (R=32, "
                          "M=100) and the modelled sweep times; orbit = H_K·v of one momentum block; grad = "
-                         "forward and backward of the differentiable 4x3 ln Z_GC (R=32, M=80)")
+                         "forward and backward of the differentiable 4x3 ln Z_GC (R=32, M=80); kresolved = k-resolved "
+                         "sector ln Z (16 orbit blocks, R=24, M=100) against the unsymmetrised batched ln Z "
+                         "(R=32, M=100) of the same sector")
     ap.add_argument("--k", type=int, nargs=2, default=(1, 2), metavar=("KX", "KY"), help="orbit workload momentum")
     return ap.parse_args()
 
@@ -472,6 +474,33 @@ def run_grad(args):
     return 0
 
 
+def run_kresolved(args):
+    """One 4x4 sector (default (5,5); U=6, V=0.5, t'=-0.25, phi=0): ln Z from the 16 momentum blocks
+    (R=24, M=100, complex128, Philox starts) and from the unsymmetrised sector (batched complex64,
+    R=32, M=100), on T = 0.1..2.0."""
+    import numpy as np
+    import torch
+    import ftlm_extended_hubbard_b200 as F
+    nu, nd = args.sector if args.sector else (5, 5)
+    p = F.HubbardParams(4, 4, 1.0, -0.25, 6.0, 0.5, 0.0, 0.0)
+    s = F.Sector(p, nu, nd)
+    T = np.round(np.arange(1, 21) * 0.1, 10)
+    bts = 1.0 / T
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lz_k, _, dims = s.orbit_ftlm(bts, 24, 100, 7, sector_index=nu * 17 + nd, start="philox")
+    t1 = time.perf_counter()
+    lz_b, _ = s.batched_ftlm(bts, 32, 100, 7)
+    t2 = time.perf_counter()
+    rel = np.abs(lz_k - lz_b) / np.abs(lz_b)
+    print(json.dumps({"workload": f"k-resolved vs unsymmetrised ln Z, 4x4 ({nu},{nd}), dim {s.dim()}",
+                      "block_dims": dims.ravel().tolist(), "T": T.tolist(), "lnz_k": lz_k.tolist(),
+                      "lnz_unsym": lz_b.tolist(), "max_rel_diff": float(rel.max()),
+                      "rel_diff_T1": float(rel[9]), "kresolved_s": t1 - t0, "batched_s": t2 - t1}))
+    F.batched_release()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -484,6 +513,8 @@ def main():
         return run_orbit(args)
     if args.workload == "grad":
         return run_grad(args)
+    if args.workload == "kresolved":
+        return run_kresolved(args)
     return run_ours(args)
 
 

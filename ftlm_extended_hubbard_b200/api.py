@@ -299,17 +299,18 @@ class Sector(_Handle):
         return OrbitKBlock(self, kx, ky)
 
     def orbit_ftlm(self, betas, n_random: int, lanczos_steps: int, seed: int, sector_index: int = 0,
-                   start: str = "reference"):
-        """k-resolved sector ln Z: every momentum block with seed + sector_index*257 + ky*17 + kx,
-        log-sum-exp over blocks.  Returns (lnz, energy, block dims [Ly][Lx])."""
+                   start: str = "reference", ed_cutoff: int = 64):
+        """k-resolved sector ln Z: blocks of dim <= ed_cutoff exactly, larger ones by FTLM with
+        seed + sector_index*257 + ky*17 + kx, log-sum-exp over blocks (the k-bench's rule; its
+        --ed-cutoff defaults to 64).  Returns (lnz, energy, block dims [Ly][Lx])."""
         bt = np.ascontiguousarray(np.atleast_1d(np.asarray(betas, dtype=np.float64)))
         lnz = np.zeros(bt.size)
         en = np.zeros(bt.size)
         Lx, Ly = (self.params.Lx, self.params.Ly) if self.params is not None else (0, 0)
         dims = np.zeros(max(1, Lx * Ly), np.int64)
         call("ftlm_gpu_orbit_sector_ftlm", self._h, bt.ctypes.data_as(C.c_void_p), bt.size, n_random, lanczos_steps,
-             C.c_uint(seed & 0xFFFFFFFF), sector_index, START_MODES[start], lnz.ctypes.data_as(C.c_void_p),
-             en.ctypes.data_as(C.c_void_p), dims.ctypes.data_as(C.c_void_p))
+             C.c_uint(seed & 0xFFFFFFFF), sector_index, START_MODES[start], ed_cutoff,
+             lnz.ctypes.data_as(C.c_void_p), en.ctypes.data_as(C.c_void_p), dims.ctypes.data_as(C.c_void_p))
         return lnz, en, dims[:Lx * Ly].reshape(Ly, Lx)
 
 

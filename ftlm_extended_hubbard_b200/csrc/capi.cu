@@ -1681,10 +1681,58 @@ int ftlm_gpu_orbit_ftlm(ftlm_orbit* o, const double* bts, int n_bt, int R, int M
   return ftlm_gpu_ftlm_combine(lq.data(), eq.data(), nv.data(), R, n_bt, std::log(static_cast<double>(dk)), lnz, energy);
 }
 
-// All momentum blocks of a sector (ky outer, kx inner), seed_k = seed + sector_index*257 + ky*17 + kx,
-// ln Z_sector = log-sum-exp over blocks (benchmarks/bench_ftlm_nmu_4x4_k.cpp:801-1081).
+// Exact ln Tr e^{-bT H_K} of a small block (the k-bench's exact_log_partition_small_complex,
+// benchmarks/bench_ftlm_nmu_4x4_k.cpp:249-333): H_K built on the GPU column by column, eigenvalues of
+// its real 2dk x 2dk embedding [[Re, -Im], [Im, Re]] (each eigenvalue twice) on the host.
+static int orbit_block_ed(ftlm_orbit* o, const double* bts, int n_bt, double* lnz, double* energy) {
+  const int64_t dk = o->dk;
+  const size_t col = static_cast<size_t>(dk) * sizeof(double2);
+  DevBuf X, Y;
+  CU_TRY(X.alloc(col * dk));
+  CU_TRY(Y.alloc(col * dk));
+  cudaStream_t st = o->sector->stream;
+  CU_TRY(cudaMemsetAsync(X.p, 0, col * dk, st));
+  const double one[2] = {1.0, 0.0};
+  for (int64_t j = 0; j < dk; ++j)
+    CU_TRY(cudaMemcpyAsync(X.as<double2>() + j * dk + j, one, sizeof(double2), cudaMemcpyHostToDevice, st));
+  for (int64_t j = 0; j < dk; ++j) {
+    const int rc = orbit_apply_dev(o, X.as<double2>() + j * dk, Y.as<double2>() + j * dk, st);
+    if (rc) return rc;
+  }
+  std::vector<double> H(static_cast<size_t>(dk) * dk * 2);  // column j = H_K e_j
+  CU_TRY(cudaMemcpyAsync(H.data(), Y.p, col * dk, cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaStreamSynchronize(st));
+  const int m = static_cast<int>(2 * dk);
+  std::vector<double> Rm(static_cast<size_t>(m) * m), lam(static_cast<size_t>(m));
+  for (int64_t j = 0; j < dk; ++j)
+    for (int64_t i = 0; i < dk; ++i) {
+      const double re = H[2 * (static_cast<size_t>(j) * dk + i)], im = H[2 * (static_cast<size_t>(j) * dk + i) + 1];
+      Rm[static_cast<size_t>(i) * m + j] = re;
+      Rm[static_cast<size_t>(i) * m + j + dk] = -im;
+      Rm[static_cast<size_t>(i + dk) * m + j] = im;
+      Rm[static_cast<size_t>(i + dk) * m + j + dk] = re;
+    }
+  const std::string err = sym_eigvals(m, Rm.data(), lam.data());
+  if (!err.empty()) return fail(FTLM_ERR_NUMERIC, err);
+  for (int b = 0; b < n_bt; ++b) {
+    double z = 0.0, ze = 0.0;
+    for (int i = 0; i < m; ++i) {
+      const double w = std::exp(-bts[b] * (lam[static_cast<size_t>(i)] - lam[0]));
+      z += w;
+      ze += w * lam[static_cast<size_t>(i)];
+    }
+    lnz[b] = std::log(0.5) - bts[b] * lam[0] + std::log(z);
+    energy[b] = ze / z;
+  }
+  return FTLM_OK;
+}
+
+// All momentum blocks of a sector (ky outer, kx inner): blocks with dim <= ed_cutoff exactly
+// (the k-bench's --ed-cutoff, default 64), larger ones by FTLM with seed_k = seed + sector_index*257 +
+// ky*17 + kx; ln Z_sector = log-sum-exp over blocks (benchmarks/bench_ftlm_nmu_4x4_k.cpp:801-1081).
 int ftlm_gpu_orbit_sector_ftlm(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed,
-                               int sector_index, int start_mode, double* lnz, double* energy, long long* dims_k) {
+                               int sector_index, int start_mode, int ed_cutoff, double* lnz, double* energy,
+                               long long* dims_k) {
   int rc = need_device(s);
   if (rc) return rc;
   if (n_bt <= 0 || !bts || !lnz || !energy) return fail(FTLM_ERR_INVALID, "bad arguments");
@@ -1701,7 +1749,11 @@ int ftlm_gpu_orbit_sector_ftlm(ftlm_sector* s, const double* bts, int n_bt, int 
       if (dims_k) dims_k[ky * s->Lx + kx] = o->dk;
       if (o->dk > 0) {
         const unsigned seed_k = seed + static_cast<unsigned>(sector_index * 257 + ky * 17 + kx);
-        rc = ftlm_gpu_orbit_ftlm(o, bts, n_bt, R, M, seed_k, start_mode, lk.data(), ek.data());
+        if (o->dk <= ed_cutoff)
+          rc = o->dk == 1 ? ftlm_gpu_orbit_ftlm(o, bts, n_bt, R, M, seed_k, start_mode, lk.data(), ek.data())
+                          : orbit_block_ed(o, bts, n_bt, lk.data(), ek.data());
+        else
+          rc = ftlm_gpu_orbit_ftlm(o, bts, n_bt, R, M, seed_k, start_mode, lk.data(), ek.data());
         if (rc) {
           ftlm_gpu_orbit_destroy(o);
           return rc;

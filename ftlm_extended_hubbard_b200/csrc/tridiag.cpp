@@ -123,4 +123,43 @@ std::string duhamel_weights(int n, const double* alpha, const double* beta, doub
   return "";
 }
 
+std::string sym_eigvals(int m, double* A, double* lam) {
+  if (m <= 0) return "";
+  auto a = [A, m](int i, int j) -> double& { return A[static_cast<size_t>(i) * m + j]; };
+  double fro = 0.0;
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < m; ++j) fro += a(i, j) * a(i, j);
+  const double stop = 1e-30 * fro;
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0;
+    for (int i = 0; i < m; ++i)
+      for (int j = i + 1; j < m; ++j) off += 2.0 * a(i, j) * a(i, j);
+    if (off <= stop) break;
+    if (sweep == 99) return "Jacobi eigenvalues did not converge";
+    for (int p = 0; p < m; ++p)
+      for (int q = p + 1; q < m; ++q) {
+        const double apq = a(p, q);
+        if (apq == 0.0) continue;
+        // rotation zeroing a(p,q): t = sgn(theta) / (|theta| + sqrt(theta^2 + 1)), theta = (a_qq - a_pp) / (2 a_pq)
+        const double theta = (a(q, q) - a(p, p)) / (2.0 * apq);
+        const double t = std::copysign(1.0, theta) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c, tau = sn / (1.0 + c);
+        a(p, p) -= t * apq;
+        a(q, q) += t * apq;
+        a(p, q) = a(q, p) = 0.0;
+        for (int r = 0; r < m; ++r) {
+          if (r == p || r == q) continue;
+          const double arp = a(r, p), arq = a(r, q);
+          const double np = arp - sn * (arq + tau * arp);
+          const double nq = arq + sn * (arp - tau * arq);
+          a(r, p) = a(p, r) = np;
+          a(r, q) = a(q, r) = nq;
+        }
+      }
+  }
+  for (int i = 0; i < m; ++i) lam[i] = a(i, i);
+  std::sort(lam, lam + m);
+  return "";
+}
+
 }  // namespace ftlm_b200

@@ -23,4 +23,9 @@ std::string tridiag_eigvec(int n, const double* alpha, const double* beta, doubl
 std::string duhamel_weights(int n, const double* alpha, const double* beta, double bT, double* K, double* g,
                             double* lam_min);
 
+// Eigenvalues (ascending) of a dense real symmetric m x m matrix A (row-major, overwritten) by
+// cyclic Jacobi rotations (Rutishauser's formulation) until the off-diagonal norm is below
+// 1e-15 of the Frobenius norm.  Returns "" or an error message.
+std::string sym_eigvals(int m, double* A, double* lam);
+
 }  // namespace ftlm_b200

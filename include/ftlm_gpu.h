@@ -220,11 +220,14 @@ int ftlm_gpu_orbit_apply_host(ftlm_orbit* o, const double* x_host, double* y_hos
 /* ftlm_log_partition_complex on one block (seed_r = seed + r*100003). */
 int ftlm_gpu_orbit_ftlm(ftlm_orbit* o, const double* bts, int n_bt, int R, int M, unsigned seed, int start_mode,
                         double* lnz, double* energy);
-/* All Lx*Ly momentum blocks of a sector with seed_k = seed + sector_index*257 + ky*17 + kx and
- * ln Z_sector = log-sum-exp over blocks (benchmarks/bench_ftlm_nmu_4x4_k.cpp:801-1081); dims_k [Lx*Ly]
- * (may be NULL) receives the block dimensions. */
+/* All Lx*Ly momentum blocks of a sector (ky outer, kx inner): blocks of dim <= ed_cutoff exactly (dense
+ * H_K, eigenvalues of its real embedding; the k-bench's --ed-cutoff, default 64), larger blocks by FTLM
+ * with seed_k = seed + sector_index*257 + ky*17 + kx; ln Z_sector = log-sum-exp over blocks
+ * (benchmarks/bench_ftlm_nmu_4x4_k.cpp:249-333, 801-1081).  dims_k [Lx*Ly] (may be NULL) receives the
+ * block dimensions. */
 int ftlm_gpu_orbit_sector_ftlm(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed,
-                               int sector_index, int start_mode, double* lnz, double* energy, long long* dims_k);
+                               int sector_index, int start_mode, int ed_cutoff, double* lnz, double* energy,
+                               long long* dims_k);
 
 /* ---- parameter gradient of the sector FTLM estimate (no counterpart in the reference) ----
  * Replays the chains of ftlm_gpu_ftlm_sector (method 0, start_mode as there) or of

@@ -7,6 +7,9 @@ published_tsv.npz  the reference's own published n(mu) tables (benchmarks/data/*
                    3x2 from the non-momentum solver; plus the per-sector ln Z lines of the 3x2 run log.
 ref_small.npz      outputs of the reference library itself (oracle/_ref): H·x on seeded vectors,
                    Lanczos alpha/beta, lanczos_extrema, and sector ln Z for small sectors.
+published_korbit.npz  the reference's published k-orbit run on 3x2 (benchmarks/data/
+                   n_vs_mu_3x2_beta20_four_solver_monitoring.txt, "solver=k-orbit" block): per-sector
+                   dim_k_total and ln Z (printed digits kept) at beta=20, R=12, M=72, seed 7, ed-cutoff 64.
 orbit_small.npz    translation-orbit momentum blocks from the reference library (OrbitKBlockBasis::build,
                    apply_orbit_k_block, ftlm_log_partition_complex): representatives, |A|, orbit sizes,
                    H_K x on seeded vectors and block ln Z.
@@ -123,6 +126,21 @@ def ref_small():
     return out
 
 
+def published_korbit():
+    txt = open(os.path.join(REF_DATA, "n_vs_mu_3x2_beta20_four_solver_monitoring.txt")).read()
+    sec = txt[txt.index("--- 3) solver=k-orbit"):]
+    rows = re.findall(r"sector \((\d+),(\d+)\) dim_full=(\d+) dim_k_total=(\d+) ed_blocks=(\d+) "
+                      r"ftlm_blocks=(\d+) logZ=(\S+)", sec)[:49]
+    assert len(rows) == 49
+    nu, nd, dfull, dk, ed, fb, lz = zip(*rows)
+    dec = [len(v.split(".")[1]) if "." in v else 0 for v in lz]
+    return {"nu": np.array(nu, np.int32), "nd": np.array(nd, np.int32), "dim_full": np.array(dfull, np.int64),
+            "dim_k_total": np.array(dk, np.int64), "ed_blocks": np.array(ed, np.int32),
+            "ftlm_blocks": np.array(fb, np.int32), "lnz": np.array([float(v) for v in lz]),
+            "decimals": np.array(dec, np.int32),
+            "params": np.array([3, 2, 1.0, -0.35, 5.75, 0.9, 20.0, 12, 72, 7, 64], np.float64)}
+
+
 ORBIT_CASES = [
     # Lx, Ly, t, tp, U, V, phix, phiy, nu, nd, kx, ky
     (2, 2, 1.0, 0.0, 4.0, 0.5, 0.0, 0.0, 2, 2, 0, 0),
@@ -195,6 +213,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "published_tsv.npz"), **published())
     np.savez_compressed(os.path.join(HERE, "ref_small.npz"), **ref_small())
     np.savez_compressed(os.path.join(HERE, "orbit_small.npz"), **orbit_small())
+    np.savez_compressed(os.path.join(HERE, "published_korbit.npz"), **published_korbit())
     np.savez_compressed(os.path.join(HERE, "config0_4x2.npz"), **config0())
     print("wrote", os.listdir(HERE))
 

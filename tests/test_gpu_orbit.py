@@ -108,7 +108,7 @@ def test_k_resolved_sector_lnz_matches_oracle(gpu):
     nu, nd, idx, seed, R, M = 2, 3, 17, 7, 6, 30
     bts = np.array([0.5, 2.0, 20.0])
     s = F.Sector(F.HubbardParams(*lat), nu, nd)
-    lz, en, dims = s.orbit_ftlm(bts, R, M, seed, sector_index=idx)
+    lz, en, dims = s.orbit_ftlm(bts, R, M, seed, sector_index=idx, ed_cutoff=0)
     so = O.OracleSector(*lat, nu, nd)
     parts = []
     for ky in range(lat[1]):
@@ -142,3 +142,19 @@ def test_orbit_rejects_bad_arguments(gpu):
     s2 = F.Sector(None, 2, 2, hops=hs, pairs=ps, n_sites=6, U=4.0, V=0.0)
     with pytest.raises(F.FtlmError):
         s2.orbit_block(0, 0)
+
+
+def test_k_resolved_sweep_reproduces_published_korbit_run(gpu, golden):
+    """All 49 sectors of the reference's published 3x2 k-orbit run (beta=20, R=12, M=72, seed 7,
+    reference start vectors, ed-cutoff 64) at printed precision where it used the orbit basis."""
+    g = golden("published_korbit.npz")
+    p = F.HubbardParams(3, 2, 1.0, -0.35, 5.75, 0.9, 0.0, 0.0)
+    for i in range(g["nu"].size):
+        nu, nd = int(g["nu"][i]), int(g["nd"][i])
+        s = F.Sector(p, nu, nd)
+        lz, _, dims = s.orbit_ftlm([20.0], 12, 72, 7, sector_index=nu * 7 + nd, ed_cutoff=64)
+        if 0 < nu < 6 and 0 < nd < 6:
+            assert dims.sum() == g["dim_k_total"][i]
+            assert abs(lz[0] - g["lnz"][i]) <= 0.6 * 10.0 ** -int(g["decimals"][i]), (nu, nd, lz[0], g["lnz"][i])
+        else:
+            assert dims.sum() == g["dim_full"][i]
