@@ -476,8 +476,9 @@ def run_grad(args):
 
 def run_kresolved(args):
     """One 4x4 sector (default (5,5); U=6, V=0.5, t'=-0.25, phi=0): ln Z from the 16 momentum blocks
-    (R=24, M=100, complex128, Philox starts) and from the unsymmetrised sector (batched complex64,
-    R=32, M=100), on T = 0.1..2.0."""
+    (R=24, M=100; batched complex64, and complex128 when dim <= 5e7) against the unsymmetrised
+    batched ln Z (R=32, M=100) of the same sector, on T = 0.1..2.0.  --sector 8 8 is the k-block
+    workload of the (8,8) sector (16 blocks of dim ~1.035e7)."""
     import numpy as np
     import torch
     import ftlm_extended_hubbard_b200 as F
@@ -486,18 +487,29 @@ def run_kresolved(args):
     s = F.Sector(p, nu, nd)
     T = np.round(np.arange(1, 21) * 0.1, 10)
     bts = 1.0 / T
+    idx = nu * 17 + nd
+    out = {"workload": f"k-resolved vs unsymmetrised ln Z, 4x4 ({nu},{nd}), dim {s.dim()}, R=24 (k) / 32, M=100",
+           "T": T.tolist()}
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    lz_k, _, dims = s.orbit_ftlm(bts, 24, 100, 7, sector_index=nu * 17 + nd, start="philox")
-    t1 = time.perf_counter()
+    lz_kb, _, dims = s.orbit_ftlm(bts, 24, 100, 7, sector_index=idx, method="batched")
+    torch.cuda.synchronize()
+    out["kresolved_batched_s"] = time.perf_counter() - t0
+    out["block_dims"] = dims.ravel().tolist()
+    out["lnz_k_batched"] = lz_kb.tolist()
+    t0 = time.perf_counter()
     lz_b, _ = s.batched_ftlm(bts, 32, 100, 7)
-    t2 = time.perf_counter()
-    rel = np.abs(lz_k - lz_b) / np.abs(lz_b)
-    print(json.dumps({"workload": f"k-resolved vs unsymmetrised ln Z, 4x4 ({nu},{nd}), dim {s.dim()}",
-                      "block_dims": dims.ravel().tolist(), "T": T.tolist(), "lnz_k": lz_k.tolist(),
-                      "lnz_unsym": lz_b.tolist(), "max_rel_diff": float(rel.max()),
-                      "rel_diff_T1": float(rel[9]), "kresolved_s": t1 - t0, "batched_s": t2 - t1}))
+    out["unsym_batched_s"] = time.perf_counter() - t0
+    out["lnz_unsym"] = lz_b.tolist()
+    out["max_abs_diff_lnz_k_vs_unsym"] = float(np.max(np.abs(lz_kb - lz_b)))
+    out["abs_diff_lnz_k_vs_unsym_T1"] = float(abs(lz_kb[9] - lz_b[9]))
     F.batched_release()
+    if s.dim() <= 50_000_000:
+        t0 = time.perf_counter()
+        lz_k, _, _ = s.orbit_ftlm(bts, 24, 100, 7, sector_index=idx, start="philox")
+        out["kresolved_complex128_s"] = time.perf_counter() - t0
+        out["max_rel_diff_batched_vs_complex128"] = float(np.max(np.abs(lz_kb - lz_k) / np.abs(lz_k)))
+    print(json.dumps(out))
     return 0
 
 

@@ -103,6 +103,8 @@ SIGNATURES = {
     "ftlm_gpu_orbit_apply_host": [_vp, _vp, _vp],
     "ftlm_gpu_orbit_ftlm": [_vp, _vp, _i, _i, _i, C.c_uint, _i, _vp, _vp],
     "ftlm_gpu_orbit_sector_ftlm": [_vp, _vp, _i, _i, _i, C.c_uint, _i, _i, _i, _vp, _vp, _vp],
+    "ftlm_gpu_orbit_batched_ftlm": [_vp, _vp, _i, _i, _i, C.c_uint, _vp, _vp],
+    "ftlm_gpu_orbit_sector_batched_ftlm": [_vp, _vp, _i, _i, _i, C.c_uint, _i, _i, _vp, _vp, _vp],
     "ftlm_gpu_gc_sweep": [C.POINTER(FtlmParams), _i, _i, C.c_uint, _i, _vp, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp],
 }
 _RESTYPES = {"ftlm_gpu_last_error": C.c_char_p, "ftlm_gpu_version_string": C.c_char_p}

@@ -299,18 +299,24 @@ class Sector(_Handle):
         return OrbitKBlock(self, kx, ky)
 
     def orbit_ftlm(self, betas, n_random: int, lanczos_steps: int, seed: int, sector_index: int = 0,
-                   start: str = "reference", ed_cutoff: int = 64):
+                   start: str = "reference", ed_cutoff: int = 64, method: str = "plain"):
         """k-resolved sector ln Z: blocks of dim <= ed_cutoff exactly, larger ones by FTLM with
         seed + sector_index*257 + ky*17 + kx, log-sum-exp over blocks (the k-bench's rule; its
-        --ed-cutoff defaults to 64).  Returns (lnz, energy, block dims [Ly][Lx])."""
+        --ed-cutoff defaults to 64).  method "batched": complex64 32-chain blocks (Philox starts).
+        Returns (lnz, energy, block dims [Ly][Lx])."""
         bt = np.ascontiguousarray(np.atleast_1d(np.asarray(betas, dtype=np.float64)))
         lnz = np.zeros(bt.size)
         en = np.zeros(bt.size)
         Lx, Ly = (self.params.Lx, self.params.Ly) if self.params is not None else (0, 0)
         dims = np.zeros(max(1, Lx * Ly), np.int64)
-        call("ftlm_gpu_orbit_sector_ftlm", self._h, bt.ctypes.data_as(C.c_void_p), bt.size, n_random, lanczos_steps,
-             C.c_uint(seed & 0xFFFFFFFF), sector_index, START_MODES[start], ed_cutoff,
-             lnz.ctypes.data_as(C.c_void_p), en.ctypes.data_as(C.c_void_p), dims.ctypes.data_as(C.c_void_p))
+        if method == "batched":
+            call("ftlm_gpu_orbit_sector_batched_ftlm", self._h, bt.ctypes.data_as(C.c_void_p), bt.size, n_random,
+                 lanczos_steps, C.c_uint(seed & 0xFFFFFFFF), sector_index, ed_cutoff, lnz.ctypes.data_as(C.c_void_p),
+                 en.ctypes.data_as(C.c_void_p), dims.ctypes.data_as(C.c_void_p))
+        else:
+            call("ftlm_gpu_orbit_sector_ftlm", self._h, bt.ctypes.data_as(C.c_void_p), bt.size, n_random,
+                 lanczos_steps, C.c_uint(seed & 0xFFFFFFFF), sector_index, START_MODES[start], ed_cutoff,
+                 lnz.ctypes.data_as(C.c_void_p), en.ctypes.data_as(C.c_void_p), dims.ctypes.data_as(C.c_void_p))
         return lnz, en, dims[:Lx * Ly].reshape(Ly, Lx)
 
 
@@ -359,6 +365,14 @@ class OrbitKBlock:
             y = np.empty_like(x)
         call("ftlm_gpu_orbit_apply_host", self._h, x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p))
         return y
+
+    def batched_ftlm(self, betas, n_random: int, lanczos_steps: int, seed: int):
+        bt = np.ascontiguousarray(np.atleast_1d(np.asarray(betas, dtype=np.float64)))
+        lnz = np.zeros(bt.size)
+        en = np.zeros(bt.size)
+        call("ftlm_gpu_orbit_batched_ftlm", self._h, bt.ctypes.data_as(C.c_void_p), bt.size, n_random, lanczos_steps,
+             C.c_uint(seed & 0xFFFFFFFF), lnz.ctypes.data_as(C.c_void_p), en.ctypes.data_as(C.c_void_p))
+        return lnz, en
 
     def ftlm(self, betas, n_random: int, lanczos_steps: int, seed: int, start: str = "reference"):
         bt = np.ascontiguousarray(np.atleast_1d(np.asarray(betas, dtype=np.float64)))

@@ -20,6 +20,7 @@
 
 #include "batched.cuh"
 #include "device.cuh"
+#include "orbit.cuh"
 
 namespace ftlm_b200 {
 
@@ -434,6 +435,148 @@ __global__ void bt_scalar_kernel(const double* __restrict__ partial, int nblocks
   st[kBtSin * 32 + lane] = 1.0 / b;
 }
 
+// Orbit momentum block, 32 chains: Y[a, :] = s_in * H_K W[a, :] (complex64 block vectors over the
+// block's representatives) and the fused <W_k, Y> per chain.  Warp per representative: the lanes
+// walk the representative's sources in the sector's gather tables 32 at a time (table lookup and
+// coefficient <rep a|H|s> eta conj(chi(R)) sqrt|A_b| / sqrt|A_a| in FP64, rounded to complex64) and
+// compact the surviving ones into the warp's shared-memory list; then the half-warps gather the
+// 256-byte rows W[b, :] as in the column pass.  Same algebra as the complex128 apply_tables kernel.
+constexpr int kOrbTerms = 256;
+
+__device__ __forceinline__ void orb_push(bool ok, uint32_t off, float2 cf, int lane, int& cnt, uint32_t* s_off,
+                                         float2* s_cf) {
+  const uint32_t m = __ballot_sync(0xffffffffu, ok);
+  if (ok) {
+    const int pos = cnt + __popc(m & ((1u << lane) - 1u));
+    s_off[pos] = off;
+    s_cf[pos] = cf;
+  }
+  cnt += __popc(m);
+}
+
+__device__ __forceinline__ float2 orb_coef(const OrbitApplyDev& A, double2 c, uint32_t e, double inv_sa) {
+  const double2 ch = A.chi_tab[(e >> 24) & 15u];
+  const double f = (((e >> 28) & 1u) ? -1.0 : 1.0) * A.sqrtA[e & 0xFFFFFFu] * inv_sa;
+  return make_float2(static_cast<float>(f * (c.x * ch.x + c.y * ch.y)), static_cast<float>(f * (c.y * ch.x - c.x * ch.y)));
+}
+
+__global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_orbit_kernel(OrbitApplyDev A, const float2* __restrict__ W,
+                                                                              float2* __restrict__ Y,
+                                                                              const double* __restrict__ st,
+                                                                              double* __restrict__ partial,
+                                                                              const int* __restrict__ flag) {
+  __shared__ uint32_t s_off[kBtWarps][kOrbTerms];
+  __shared__ float2 s_cf[kBtWarps][kOrbTerms];
+  __shared__ double sh[4 * kBtThreads];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int hv = lane >> 4, l = lane & 15;
+  const float4 sc = make_float4(static_cast<float>(st[kBtSin * 32 + 2 * l]), 0.f,
+                                static_cast<float>(st[kBtSin * 32 + 2 * l + 1]), 0.f);
+  const bool filter = *flag != 0;
+  const DevSector& S = A.S;
+  const int64_t Dd = S.Dd;
+  const float4* W4 = reinterpret_cast<const float4*>(W);
+  float4* Y4 = reinterpret_cast<float4*>(Y);
+  uint32_t* off = s_off[warp];
+  float2* cfs = s_cf[warp];
+  constexpr uint32_t kNone = 0xFFFFFFFFu;
+  double d0r = 0.0, d0i = 0.0, d1r = 0.0, d1i = 0.0;
+  for (int64_t a = static_cast<int64_t>(blockIdx.x) * kBtWarps + warp; a < A.dk;
+       a += static_cast<int64_t>(gridDim.x) * kBtWarps) {
+    const uint32_t pk = A.reps[a];
+    const uint32_t u = pk >> 16, d = pk & 0xFFFFu;
+    const int32_t ru = A.O.rank_u[u], rd = A.O.rank_d[d];
+    const double inv_sa = 1.0 / A.sqrtA[a];
+    int cnt = 0;
+    __syncwarp();
+    const uint32_t q = prefix_parity_shifted(d);
+    const int p1 = S.up_ptr[ru + 1];
+    for (int p0 = S.up_ptr[ru]; p0 < p1; p0 += 32) {
+      const int p = p0 + lane;
+      bool ok = false;
+      uint32_t o = 0;
+      float2 cf = make_float2(0.f, 0.f);
+      if (p < p1) {
+        const uint32_t e = __ldg(A.table + static_cast<int64_t>(S.up_src[p]) * Dd + rd);
+        if (e != kNone) {
+          const uint32_t lh = S.up_lohi[p];
+          double2 c = S.up_coef[p];
+          if (((q >> (lh & 255u)) ^ (q >> (lh >> 8))) & 1u) c = make_double2(-c.x, -c.y);
+          ok = true;
+          o = (e & 0xFFFFFFu) * 16u;
+          cf = orb_coef(A, c, e, inv_sa);
+        }
+      }
+      orb_push(ok, o, cf, lane, cnt, off, cfs);
+    }
+    const int64_t rowbase = static_cast<int64_t>(ru) * Dd;
+    const int64_t d1 = S.dn_csr_ptr[rd + 1];
+    for (int64_t p0 = S.dn_csr_ptr[rd]; p0 < d1; p0 += 32) {
+      const int64_t p = p0 + lane;
+      bool ok = false;
+      uint32_t o = 0;
+      float2 cf = make_float2(0.f, 0.f);
+      if (p < d1) {
+        const uint32_t ent = S.dn_csr_ent[p];
+        const int h = static_cast<int>((ent >> 1) & 255u);
+        if (h != S.n_dn_hops) {
+          const uint32_t e = __ldg(A.table + rowbase + (ent >> 9));
+          if (e != kNone) {
+            double2 c = S.dn_coef[h];
+            if ((ent & 1u) ^ (static_cast<uint32_t>(__popc(u & S.dn_nmask[h])) & 1u)) c = make_double2(-c.x, -c.y);
+            ok = true;
+            o = (e & 0xFFFFFFu) * 16u;
+            cf = orb_coef(A, c, e, inv_sa);
+          }
+        }
+      }
+      orb_push(ok, o, cf, lane, cnt, off, cfs);
+    }
+    const int deg8 = (cnt + 7) & ~7;
+    for (int j = cnt + lane; j < deg8; j += 32) {  // padding: a valid row, zero coefficient
+      off[j] = static_cast<uint32_t>(a) * 16u;
+      cfs[j] = make_float2(0.f, 0.f);
+    }
+    __syncwarp();
+    const float4* Wc = W4 + l;
+    const float4 acc = filter ? bt_cols_sum<true>(Wc, off, cfs, deg8, hv) : bt_cols_sum<false>(Wc, off, cfs, deg8, hv);
+    if (hv == 0) {
+      float4 w = W4[static_cast<uint32_t>(a) * 16u + l];
+      const float4 wf = filter ? filt4(w) : w;
+      const float dg = static_cast<float>(diag_value(S, u, d, S.cnt_uu[ru], S.cnt_dd[rd], S.wpl[ru]));
+      float4 y;
+      y.x = (acc.x + dg * wf.x) * sc.x;
+      y.y = (acc.y + dg * wf.y) * sc.x;
+      y.z = (acc.z + dg * wf.z) * sc.z;
+      y.w = (acc.w + dg * wf.w) * sc.z;
+      Y4[static_cast<uint32_t>(a) * 16u + l] = y;
+      const double wx = w.x, wy = w.y, wz = w.z, ww = w.w;
+      const double yx = y.x, yy = y.y, yz = y.z, yw = y.w;
+      d0r = fma(wx, yx, fma(wy, yy, d0r));
+      d0i = fma(wx, yy, fma(-wy, yx, d0i));
+      d1r = fma(wz, yz, fma(ww, yw, d1r));
+      d1i = fma(wz, yw, fma(-ww, yz, d1i));
+    }
+  }
+  const int t = threadIdx.x;
+  sh[0 * kBtThreads + t] = d0r;
+  sh[1 * kBtThreads + t] = d0i;
+  sh[2 * kBtThreads + t] = d1r;
+  sh[3 * kBtThreads + t] = d1i;
+  __syncthreads();
+  if (t < 32) {
+    const int ll = t & 15, which = t >> 4;
+    double re = 0.0, im = 0.0;
+    for (int w = 0; w < kBtWarps; ++w) {
+      re += sh[(2 * which) * kBtThreads + w * 32 + ll];
+      im += sh[(2 * which + 1) * kBtThreads + w * 32 + ll];
+    }
+    const int chain = 2 * ll + which;
+    partial[(blockIdx.x * 32 + chain) * 2] = re;
+    partial[(blockIdx.x * 32 + chain) * 2 + 1] = im;
+  }
+}
+
 }  // namespace
 
 cudaError_t bt_start(float2* W, int64_t dim, unsigned seed, double* st, double* partial, int* used, int* flags,
@@ -456,6 +599,19 @@ cudaError_t bt_step(const DevSector& S, const float2* Wk, const float2* Wkm1, fl
   bt_cols_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(S, Wk, Y, st, partial, fin);
   bt_scalar_kernel<<<1, 32, 0, s>>>(partial, kBtBlocks, 1, k, st, alpha, beta, used);
   bt_update_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(Y, Wk, Wkm1, S.dim, st, k > 0, partial, fout);
+  bt_scalar_kernel<<<1, 32, 0, s>>>(partial, kBtBlocks, 2, k, st, alpha, beta, used);
+  return cudaGetLastError();
+}
+
+cudaError_t bt_orbit_step(const OrbitApplyDev& A, const float2* Wk, const float2* Wkm1, float2* Y, int k, double* st,
+                          double* partial, double* alpha, double* beta, int* used, int* flags, cudaStream_t s) {
+  int* fin = flags + (k & 1);
+  int* fout = flags + ((k + 1) & 1);
+  cudaError_t e = cudaMemsetAsync(fout, 0, sizeof(int), s);
+  if (e != cudaSuccess) return e;
+  bt_orbit_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(A, Wk, Y, st, partial, fin);
+  bt_scalar_kernel<<<1, 32, 0, s>>>(partial, kBtBlocks, 1, k, st, alpha, beta, used);
+  bt_update_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(Y, Wk, Wkm1, A.dk, st, k > 0, partial, fout);
   bt_scalar_kernel<<<1, 32, 0, s>>>(partial, kBtBlocks, 2, k, st, alpha, beta, used);
   return cudaGetLastError();
 }

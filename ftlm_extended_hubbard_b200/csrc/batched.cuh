@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include "device.cuh"
+#include "orbit.cuh"
 
 namespace ftlm_b200 {
 
@@ -26,6 +27,12 @@ cudaError_t bt_start(float2* W, int64_t dim, unsigned seed, double* st, double* 
 // One Lanczos step k for all chains: Y <- H q_k, z, W_{k+1} (into Y), beta_k; alpha/beta [M][32].
 cudaError_t bt_step(const DevSector& S, const float2* Wk, const float2* Wkm1, float2* Y, int k, double* st,
                     double* partial, double* alpha, double* beta, int* used, int* flags, cudaStream_t s);
+
+// One Lanczos step for 32 chains of an orbit momentum block (block vectors over its dk
+// representatives); same contract as bt_step.  Needs the sector's max up-degree <= 120 and at most
+// 256 sources per representative.
+cudaError_t bt_orbit_step(const OrbitApplyDev& A, const float2* Wk, const float2* Wkm1, float2* Y, int k, double* st,
+                          double* partial, double* alpha, double* beta, int* used, int* flags, cudaStream_t s);
 
 // Y = H X for one block vector, without Lanczos bookkeeping: st_unit holds kBtSin = 1 for every
 // chain, zero_flag points to an int 0 (no small-entry filter), partial receives unused dot sums.

@@ -862,15 +862,14 @@ GradWs g_grad;
 
 
 // Runs ceil(R/32) blocks of 32 chains on sector s; A/B [R][M] (beta zero-padded), used [R].
-int bt_run_chains(ftlm_sector* s, int R, int M, unsigned seed, std::vector<double>* A, std::vector<double>* B,
-                  std::vector<int>* used) {
-  const int64_t dim = s->plan.dim;
+template <class Step>
+int bt_run_chains_impl(int64_t dim, cudaStream_t st, Step&& step, int R, int M, unsigned seed, std::vector<double>* A,
+                       std::vector<double>* B, std::vector<int>* used) {
   A->assign(static_cast<size_t>(R) * M, 0.0);
   B->assign(static_cast<size_t>(R) * M, 0.0);
   used->assign(static_cast<size_t>(R), 0);
   std::lock_guard<std::mutex> lock(g_bt_mu);
   CU_TRY(g_bt.ensure(dim, M));
-  cudaStream_t st = s->stream;
   float2* bufs[3] = {g_bt.buf[0].as<float2>(), g_bt.buf[1].as<float2>(), g_bt.buf[2].as<float2>()};
   double* sd = g_bt.st.as<double>();
   double* part = g_bt.partial.as<double>();
@@ -890,7 +889,7 @@ int bt_run_chains(ftlm_sector* s, int R, int M, unsigned seed, std::vector<doubl
     float2 *wk = bufs[0], *y = bufs[1], *wkm1 = bufs[2];
     cudaError_t ce = cudaSuccess;
     for (int k = 0; k < M && ce == cudaSuccess; ++k) {
-      ce = bt_step(s->dev, wk, wkm1, y, k, sd, part, al, be, us, fl, st);
+      ce = step(wk, wkm1, y, k, sd, part, al, be, us, fl);
       float2* t = wkm1;
       wkm1 = wk;
       wk = y;
@@ -925,6 +924,17 @@ int bt_run_chains(ftlm_sector* s, int R, int M, unsigned seed, std::vector<doubl
     }
   }
   return FTLM_OK;
+}
+
+int bt_run_chains(ftlm_sector* s, int R, int M, unsigned seed, std::vector<double>* A, std::vector<double>* B,
+                  std::vector<int>* used) {
+  cudaStream_t st = s->stream;
+  const DevSector& S = s->dev;
+  return bt_run_chains_impl(
+      s->plan.dim, st,
+      [&S, st](const float2* wk, const float2* wkm1, float2* y, int k, double* sd, double* part, double* al, double* be,
+               int* us, int* fl) { return bt_step(S, wk, wkm1, y, k, sd, part, al, be, us, fl, st); },
+      R, M, seed, A, B, used);
 }
 
 }  // namespace
@@ -1681,6 +1691,36 @@ int ftlm_gpu_orbit_ftlm(ftlm_orbit* o, const double* bts, int n_bt, int R, int M
   return ftlm_gpu_ftlm_combine(lq.data(), eq.data(), nv.data(), R, n_bt, std::log(static_cast<double>(dk)), lnz, energy);
 }
 
+// Batched complex64 FTLM of one block: 32-chain blocks of bt_orbit_step (Philox starts, as the
+// sector path); blocks with dim <= 2M use the complex128 Philox path.
+int ftlm_gpu_orbit_batched_ftlm(ftlm_orbit* o, const double* bts, int n_bt, int R, int M, unsigned seed, double* lnz,
+                                double* energy) {
+  if (!o) return fail(FTLM_ERR_INVALID, "null orbit");
+  if (n_bt < 0 || (n_bt > 0 && (!bts || !lnz || !energy))) return fail(FTLM_ERR_INVALID, "bad arguments");
+  R = std::max(1, R);
+  M = std::max(1, M);
+  if (M > 160) return fail(FTLM_ERR_UNSUPPORTED, "more than 160 Lanczos steps for the on-chip Jacobi");
+  const int64_t dk = o->dk;
+  if (dk <= 2 * static_cast<int64_t>(M)) return ftlm_gpu_orbit_ftlm(o, bts, n_bt, R, M, seed, FTLM_START_PHILOX, lnz, energy);
+  const SectorPlan& P = o->sector->plan;
+  if (P.max_up_deg > 120 || P.max_up_deg + ((P.max_dn_deg + 7) / 8) * 8 + 8 > 256)
+    return fail(FTLM_ERR_UNSUPPORTED, "batched orbit path: more than 256 sources per representative");
+  cudaStream_t st = o->sector->stream;
+  const OrbitApplyDev& Adev = o->app;
+  std::vector<double> A, B;
+  std::vector<int> used;
+  int rc = bt_run_chains_impl(
+      dk, st,
+      [&Adev, st](const float2* wk, const float2* wkm1, float2* y, int k, double* sd, double* part, double* al,
+                  double* be, int* us, int* fl) { return bt_orbit_step(Adev, wk, wkm1, y, k, sd, part, al, be, us, fl, st); },
+      R, M, seed, &A, &B, &used);
+  if (rc) return rc;
+  std::vector<double> lq(static_cast<size_t>(R) * n_bt), eq(static_cast<size_t>(R) * n_bt);
+  rc = ftlm_gpu_tridiag_quadrature(A.data(), B.data(), used.data(), R, M, bts, n_bt, lq.data(), eq.data());
+  if (rc) return rc;
+  return ftlm_gpu_ftlm_combine(lq.data(), eq.data(), used.data(), R, n_bt, std::log(static_cast<double>(dk)), lnz, energy);
+}
+
 // Exact ln Tr e^{-bT H_K} of a small block (the k-bench's exact_log_partition_small_complex,
 // benchmarks/bench_ftlm_nmu_4x4_k.cpp:249-333): H_K built on the GPU column by column, eigenvalues of
 // its real 2dk x 2dk embedding [[Re, -Im], [Im, Re]] (each eigenvalue twice) on the host.
@@ -1730,9 +1770,9 @@ static int orbit_block_ed(ftlm_orbit* o, const double* bts, int n_bt, double* ln
 // All momentum blocks of a sector (ky outer, kx inner): blocks with dim <= ed_cutoff exactly
 // (the k-bench's --ed-cutoff, default 64), larger ones by FTLM with seed_k = seed + sector_index*257 +
 // ky*17 + kx; ln Z_sector = log-sum-exp over blocks (benchmarks/bench_ftlm_nmu_4x4_k.cpp:801-1081).
-int ftlm_gpu_orbit_sector_ftlm(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed,
-                               int sector_index, int start_mode, int ed_cutoff, double* lnz, double* energy,
-                               long long* dims_k) {
+static int orbit_sector_impl(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed,
+                             int sector_index, int start_mode, int ed_cutoff, bool batched, double* lnz, double* energy,
+                             long long* dims_k) {
   int rc = need_device(s);
   if (rc) return rc;
   if (n_bt <= 0 || !bts || !lnz || !energy) return fail(FTLM_ERR_INVALID, "bad arguments");
@@ -1752,6 +1792,8 @@ int ftlm_gpu_orbit_sector_ftlm(ftlm_sector* s, const double* bts, int n_bt, int 
         if (o->dk <= ed_cutoff)
           rc = o->dk == 1 ? ftlm_gpu_orbit_ftlm(o, bts, n_bt, R, M, seed_k, start_mode, lk.data(), ek.data())
                           : orbit_block_ed(o, bts, n_bt, lk.data(), ek.data());
+        else if (batched)
+          rc = ftlm_gpu_orbit_batched_ftlm(o, bts, n_bt, R, M, seed_k, lk.data(), ek.data());
         else
           rc = ftlm_gpu_orbit_ftlm(o, bts, n_bt, R, M, seed_k, start_mode, lk.data(), ek.data());
         if (rc) {
@@ -1777,6 +1819,18 @@ int ftlm_gpu_orbit_sector_ftlm(ftlm_sector* s, const double* bts, int n_bt, int 
   std::copy(acc.begin(), acc.end(), lnz);
   std::copy(eacc.begin(), eacc.end(), energy);
   return FTLM_OK;
+}
+
+int ftlm_gpu_orbit_sector_ftlm(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed,
+                               int sector_index, int start_mode, int ed_cutoff, double* lnz, double* energy,
+                               long long* dims_k) {
+  return orbit_sector_impl(s, bts, n_bt, R, M, seed, sector_index, start_mode, ed_cutoff, false, lnz, energy, dims_k);
+}
+
+int ftlm_gpu_orbit_sector_batched_ftlm(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed,
+                                       int sector_index, int ed_cutoff, double* lnz, double* energy, long long* dims_k) {
+  return orbit_sector_impl(s, bts, n_bt, R, M, seed, sector_index, FTLM_START_PHILOX, ed_cutoff, true, lnz, energy,
+                           dims_k);
 }
 
 }  // extern "C"

@@ -228,6 +228,12 @@ int ftlm_gpu_orbit_ftlm(ftlm_orbit* o, const double* bts, int n_bt, int R, int M
 int ftlm_gpu_orbit_sector_ftlm(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed,
                                int sector_index, int start_mode, int ed_cutoff, double* lnz, double* energy,
                                long long* dims_k);
+/* The same with complex64 32-chain blocks (FP64 scalars, Philox starts, the batched sector path's
+ * rules; blocks with dim <= 2M on the complex128 Philox path).  ftlm_gpu_orbit_batched_ftlm: one block. */
+int ftlm_gpu_orbit_batched_ftlm(ftlm_orbit* o, const double* bts, int n_bt, int R, int M, unsigned seed, double* lnz,
+                                double* energy);
+int ftlm_gpu_orbit_sector_batched_ftlm(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed,
+                                       int sector_index, int ed_cutoff, double* lnz, double* energy, long long* dims_k);
 
 /* ---- parameter gradient of the sector FTLM estimate (no counterpart in the reference) ----
  * Replays the chains of ftlm_gpu_ftlm_sector (method 0, start_mode as there) or of

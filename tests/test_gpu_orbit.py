@@ -158,3 +158,25 @@ def test_k_resolved_sweep_reproduces_published_korbit_run(gpu, golden):
             assert abs(lz[0] - g["lnz"][i]) <= 0.6 * 10.0 ** -int(g["decimals"][i]), (nu, nd, lz[0], g["lnz"][i])
         else:
             assert dims.sum() == g["dim_full"][i]
+
+
+@pytest.mark.parametrize("nu,nd,k", [(4, 4, (1, 2)), (3, 3, (0, 0)), (5, 3, (2, 3))])
+def test_batched_orbit_ftlm_follows_complex128(gpu, nu, nd, k):
+    """complex64 32-chain blocks of one momentum block against the complex128 chains with the same
+    Philox start vectors: block ln Z within 1e-6 relative."""
+    s = F.Sector(F.HubbardParams(4, 4, 1.0, -0.25, 6.0, 0.5, 0.0, 0.0), nu, nd)
+    o = s.orbit_block(*k)
+    bts = 1.0 / np.array([0.1, 0.5, 1.0, 2.0])
+    lz_b, e_b = o.batched_ftlm(bts, 32, 60, 11)
+    lz_p, e_p = o.ftlm(bts, 32, 60, 11, start="philox")
+    assert np.all(np.abs(lz_b - lz_p) <= 1e-6 * np.abs(lz_p)), (lz_b, lz_p)
+    assert np.all(np.abs(e_b - e_p) <= 1e-6 * np.maximum(1.0, np.abs(e_p)))
+
+
+def test_batched_k_resolved_sector_follows_complex128(gpu):
+    s = F.Sector(F.HubbardParams(4, 3, 1.0, -0.25, 8.0, 1.0, 0.0, 0.0), 4, 3)
+    bts = 1.0 / np.array([0.2, 1.0])
+    lz_b, _, d1 = s.orbit_ftlm(bts, 24, 60, 7, sector_index=68, method="batched")
+    lz_p, _, d2 = s.orbit_ftlm(bts, 24, 60, 7, sector_index=68, start="philox")
+    assert np.array_equal(d1, d2)
+    assert np.all(np.abs(lz_b - lz_p) <= 1e-6 * np.abs(lz_p)), (lz_b, lz_p)
