@@ -1,0 +1,305 @@
+#include "capi_internal.hpp"
+
+using namespace ftlm_b200;
+using namespace ftlm_b200::capi;
+
+// ---------------------------------------------------------------------------------------------
+// Parameter gradient of the sector FTLM estimate (no reference counterpart).
+//
+// For one chain with normalised start vector r, Lanczos vectors q_i and tridiagonal T, the
+// estimator term is g = e_1^T e^{-bT T} e_1 and, with r fixed, its exact derivative in the Krylov
+// space is dg/dtheta = -sum_il K_il <q_i| dH/dtheta |q_l> (Duhamel; K from duhamel_weights).  The
+// chains are replayed from their seed with the forward's kernels (bit-identical alpha/beta), the
+// vectors kept on the device, and the three moments of dH/dU (double occupancy), dH/dV (neighbour
+// pair density) and dH/dt' (the t' hopping operator) reduced by grad.cu.
+namespace {
+
+struct ChainGrad {
+  bool ok = false;
+  double lmin = 0.0, g = 0.0, m[3] = {0.0, 0.0, 0.0};
+};
+
+// Weight matrices of up to nc chains, layout [i][ld][nc] (chain fastest), scales 1/(b_i b_l).
+int fill_weights(int nc, int ld, double bT, const std::vector<int>& n, const std::vector<double>& A,
+                 const std::vector<double>& B, const std::vector<std::vector<double>>& scale, std::vector<double>* Kp,
+                 std::vector<ChainGrad>* out) {
+  Kp->assign(static_cast<size_t>(ld) * ld * nc, 0.0);
+  std::vector<double> K;
+  for (int c = 0; c < nc; ++c) {
+    const int nn = n[static_cast<size_t>(c)];
+    ChainGrad& cg = (*out)[static_cast<size_t>(c)];
+    cg = ChainGrad{};
+    if (nn <= 0) continue;
+    K.assign(static_cast<size_t>(nn) * nn, 0.0);
+    const std::string err = duhamel_weights(nn, A.data() + static_cast<size_t>(c) * ld, B.data() + static_cast<size_t>(c) * ld,
+                                            bT, K.data(), &cg.g, &cg.lmin);
+    if (!err.empty()) return fail(FTLM_ERR_NUMERIC, err);
+    cg.ok = true;
+    const std::vector<double>& sc = scale[static_cast<size_t>(c)];
+    for (int i = 0; i < nn; ++i)
+      for (int l = 0; l < nn; ++l)
+        (*Kp)[(static_cast<size_t>(i) * ld + l) * nc + c] =
+            K[static_cast<size_t>(i) * nn + l] / (sc[static_cast<size_t>(i)] * sc[static_cast<size_t>(l)]);
+  }
+  return FTLM_OK;
+}
+
+// Moments of one batch of chains: Q [n][vstride], AQ likewise (or null), Kp [n][ld][nc].
+template <class T>
+int run_moments(ftlm_sector* s, const T* Q, const T* AQ, int64_t vstride, const std::vector<double>& Kp, int n, int ld,
+                int nc, std::vector<ChainGrad>* out) {
+  cudaStream_t st = s->stream;
+  CU_TRY(g_grad.grow(g_grad.Kp, g_grad.kcap, Kp.size() * sizeof(double)));
+  CU_TRY(cudaMemcpyAsync(g_grad.Kp.p, Kp.data(), Kp.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  CU_TRY(g_grad.grow(g_grad.part, g_grad.pcap, static_cast<size_t>(2048) * 32 * 3 * sizeof(double)));
+  int grid = 0;
+  cudaError_t e;
+  if constexpr (sizeof(T) == sizeof(float2))
+    e = grad_moments_c64(s->dev, Q, AQ ? AQ : Q, vstride, g_grad.Kp.as<double>(), n, ld, g_grad.part.as<double>(), &grid, st);
+  else
+    e = grad_moments_c128(s->dev, Q, AQ ? AQ : Q, vstride, g_grad.Kp.as<double>(), n, ld, g_grad.part.as<double>(), &grid,
+                          st);
+  if (e == cudaErrorInvalidValue)
+    return fail(FTLM_ERR_UNSUPPORTED, "gradient: Lanczos vectors of one block do not fit in shared memory");
+  CU_TRY(e);
+  std::vector<double> hp(static_cast<size_t>(grid) * nc * 3);
+  CU_TRY(cudaMemcpyAsync(hp.data(), g_grad.part.p, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaStreamSynchronize(st));
+  for (int c = 0; c < nc; ++c) {
+    ChainGrad& cg = (*out)[static_cast<size_t>(c)];
+    for (int q = 0; q < 3; ++q) {
+      double sum = 0.0;
+      for (int b = 0; b < grid; ++b) sum += hp[(static_cast<size_t>(b) * nc + c) * 3 + q];
+      cg.m[q] = sum;
+    }
+  }
+  return FTLM_OK;
+}
+
+// Plain path: complex128 chains of ftlm_gpu_ftlm_sector (seed_r = seed + r*100003).
+int grad_plain(ftlm_sector* s, ftlm_sector* op, double bT, int R, int M, unsigned seed, int start_mode,
+               std::vector<ChainGrad>* out) {
+  const int64_t dim = s->plan.dim;
+  CU_TRY(g_grad.grow(g_grad.Q, g_grad.qcap, static_cast<size_t>(M) * dim * sizeof(double2)));
+  if (op) CU_TRY(g_grad.grow(g_grad.AQ, g_grad.acap, static_cast<size_t>(M) * dim * sizeof(double2)));
+  double2* Q = g_grad.Q.as<double2>();
+  double2* AQ = op ? g_grad.AQ.as<double2>() : nullptr;
+  out->assign(static_cast<size_t>(R), ChainGrad{});
+  std::vector<ChainGrad> one(1);
+  for (int r = 0; r < R; ++r) {
+    std::vector<double> a, b;
+    int rc = run_lanczos(
+        dim, [s](const double2* x, double2* y, cudaStream_t st) { return s->apply(x, y, st); }, s->ws, M,
+        seed + static_cast<unsigned>(r) * 100003u, start_mode, s->stream, &a, &b, Q);
+    if (rc) return rc;
+    const int n = static_cast<int>(a.size());
+    if (n <= 0) continue;
+    std::vector<double> A(static_cast<size_t>(M), 0.0), B(static_cast<size_t>(M), 0.0);
+    std::copy(a.begin(), a.end(), A.begin());
+    std::copy(b.begin(), b.begin() + std::min<size_t>(b.size(), static_cast<size_t>(M)), B.begin());
+    if (op)
+      for (int i = 0; i < n; ++i) {
+        rc = op->apply(Q + static_cast<int64_t>(i) * dim, AQ + static_cast<int64_t>(i) * dim, s->stream);
+        if (rc) return rc;
+      }
+    std::vector<double> Kp;
+    std::vector<std::vector<double>> scale(1, std::vector<double>(static_cast<size_t>(n), 1.0));
+    rc = fill_weights(1, M, bT, std::vector<int>{n}, A, B, scale, &Kp, &one);
+    if (rc) return rc;
+    rc = run_moments<double2>(s, Q, AQ, dim, Kp, n, M, 1, &one);
+    if (rc) return rc;
+    (*out)[static_cast<size_t>(r)] = one[0];
+  }
+  return FTLM_OK;
+}
+
+// Batched path: complex64 32-chain blocks of ftlm_gpu_batched_ftlm_sector, replayed step by step.
+int grad_batched(ftlm_sector* s, ftlm_sector* op, double bT, int R, int M, unsigned seed, std::vector<ChainGrad>* out) {
+  const int64_t dim = s->plan.dim;
+  const int64_t vs = dim * kBtChains;
+  std::lock_guard<std::mutex> lock(g_bt_mu);
+  CU_TRY(g_bt.ensure(dim, M));
+  CU_TRY(g_grad.grow(g_grad.Q, g_grad.qcap, static_cast<size_t>(M + 1) * vs * sizeof(float2)));
+  if (op) CU_TRY(g_grad.grow(g_grad.AQ, g_grad.acap, static_cast<size_t>(M) * vs * sizeof(float2)));
+  if (!g_grad.stunit.p) {
+    std::vector<double> unit(static_cast<size_t>(kBtFields) * kBtChains, 0.0);
+    for (int c = 0; c < kBtChains; ++c) unit[static_cast<size_t>(kBtSin) * kBtChains + c] = 1.0;
+    CU_TRY(g_grad.stunit.alloc(unit.size() * sizeof(double)));
+    CU_TRY(cudaMemcpy(g_grad.stunit.p, unit.data(), unit.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CU_TRY(g_grad.zflag.alloc(sizeof(int)));
+    CU_TRY(cudaMemset(g_grad.zflag.p, 0, sizeof(int)));
+  }
+  cudaStream_t st = s->stream;
+  float2* Q = g_grad.Q.as<float2>();
+  float2* AQ = op ? g_grad.AQ.as<float2>() : nullptr;
+  double* sd = g_bt.st.as<double>();
+  double* part = g_bt.partial.as<double>();
+  double* al = g_bt.alpha.as<double>();
+  double* be = g_bt.beta.as<double>();
+  int* us = g_bt.used.as<int>();
+  int* fl = g_bt.flags.as<int>();
+  out->assign(static_cast<size_t>(R), ChainGrad{});
+  std::vector<double> ha(static_cast<size_t>(M) * kBtChains), hb(static_cast<size_t>(M) * kBtChains),
+      hs(static_cast<size_t>(kBtFields) * kBtChains);
+  std::vector<int> hu(kBtChains);
+  for (int blk = 0; blk * kBtChains < R; ++blk) {
+    const unsigned seed_b = seed + static_cast<unsigned>(blk * kBtChains) * 100003u;
+    CU_TRY(cudaMemsetAsync(al, 0, static_cast<size_t>(M) * kBtChains * sizeof(double), st));
+    CU_TRY(cudaMemsetAsync(be, 0, static_cast<size_t>(M) * kBtChains * sizeof(double), st));
+    CU_TRY(bt_start(Q, dim, seed_b, sd, part, us, fl, st));
+    CU_TRY(cudaMemcpyAsync(hs.data(), sd, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    for (int k = 0; k < M; ++k)
+      CU_TRY(bt_step(s->dev, Q + static_cast<int64_t>(k) * vs, Q + static_cast<int64_t>(k > 0 ? k - 1 : 0) * vs,
+                     Q + static_cast<int64_t>(k + 1) * vs, k, sd, part, al, be, us, fl, st));
+    CU_TRY(cudaMemcpyAsync(ha.data(), al, ha.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CU_TRY(cudaMemcpyAsync(hb.data(), be, hb.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CU_TRY(cudaMemcpyAsync(hu.data(), us, hu.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CU_TRY(cudaStreamSynchronize(st));
+    const int nc = std::min(kBtChains, R - blk * kBtChains);
+    std::vector<int> n(static_cast<size_t>(kBtChains), 0);
+    std::vector<double> A(static_cast<size_t>(kBtChains) * M, 0.0), B(static_cast<size_t>(kBtChains) * M, 0.0);
+    std::vector<std::vector<double>> scale(static_cast<size_t>(kBtChains));
+    int nmax = 0;
+    for (int c = 0; c < nc; ++c) {
+      const double sin0 = hs[static_cast<size_t>(kBtSin) * kBtChains + c];
+      const int nn = (sin0 > 0.0) ? hu[static_cast<size_t>(c)] : 0;
+      n[static_cast<size_t>(c)] = nn;
+      nmax = std::max(nmax, nn);
+      auto& sc = scale[static_cast<size_t>(c)];
+      sc.assign(static_cast<size_t>(std::max(nn, 1)), 1.0);
+      for (int k = 0; k < M; ++k) {
+        A[static_cast<size_t>(c) * M + k] = ha[static_cast<size_t>(k) * kBtChains + c];
+        B[static_cast<size_t>(c) * M + k] = hb[static_cast<size_t>(k) * kBtChains + c];
+      }
+      if (nn > 0) {  // W_0 = ||raw|| q_0, W_i = beta_{i-1} q_i
+        sc[0] = 1.0 / sin0;
+        for (int i = 1; i < nn; ++i) sc[static_cast<size_t>(i)] = B[static_cast<size_t>(c) * M + i - 1];
+      }
+    }
+    if (nmax == 0) continue;
+    if (op)
+      for (int i = 0; i < nmax; ++i)
+        CU_TRY(bt_apply(op->dev, Q + static_cast<int64_t>(i) * vs, AQ + static_cast<int64_t>(i) * vs,
+                        g_grad.stunit.as<double>(), part, g_grad.zflag.as<int>(), st));
+    std::vector<double> Kp;
+    std::vector<ChainGrad> cg(static_cast<size_t>(kBtChains));
+    int rc = fill_weights(kBtChains, M, bT, n, A, B, scale, &Kp, &cg);
+    if (rc) return rc;
+    rc = run_moments<float2>(s, Q, AQ, vs, Kp, nmax, M, kBtChains, &cg);
+    if (rc) return rc;
+    for (int c = 0; c < nc; ++c) (*out)[static_cast<size_t>(blk * kBtChains + c)] = cg[static_cast<size_t>(c)];
+  }
+  return FTLM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ftlm_gpu_grad_sector(ftlm_sector* s, ftlm_sector* op_tp, double bT, int R, int M, unsigned seed, int method,
+                         int start_mode, double* lnz, double* dlnz) {
+  int rc = need_device(s);
+  if (rc) return rc;
+  if (op_tp) {
+    rc = need_device(op_tp);
+    if (rc) return rc;
+    if (op_tp->plan.n != s->plan.n || op_tp->plan.nu != s->plan.nu || op_tp->plan.nd != s->plan.nd)
+      return fail(FTLM_ERR_INVALID, "gradient operator sector has a different (n_sites, N_up, N_dn)");
+  }
+  if (!lnz || !dlnz || method < 0 || method > 1) return fail(FTLM_ERR_INVALID, "bad arguments");
+  R = std::max(1, R);
+  M = std::max(1, M);
+  const int64_t dim = s->plan.dim;
+  std::vector<ChainGrad> cg;
+  if (method == 1 && dim > 2 * static_cast<int64_t>(M)) {
+    if (s->plan.max_up_deg > 120 || (op_tp && op_tp->plan.max_up_deg > 120))
+      return fail(FTLM_ERR_UNSUPPORTED, "batched path: more than 120 up-hop sources per string");
+    rc = grad_batched(s, op_tp, bT, R, M, seed, &cg);
+  } else {
+    rc = grad_plain(s, op_tp, bT, R, M, seed, method == 1 ? FTLM_START_PHILOX : start_mode, &cg);
+  }
+  if (rc) return rc;
+  // ln Z = ln dim + log mean_r g_r, g_r = e^{-bT lmin_r} ghat_r; d ln Z = -sum_r e^{-bT lmin_r} m_r / sum_r g_r
+  double mx = -std::numeric_limits<double>::infinity();
+  int used = 0;
+  for (const auto& c : cg)
+    if (c.ok) {
+      mx = std::max(mx, -bT * c.lmin + std::log(c.g));
+      ++used;
+    }
+  if (used == 0) {
+    *lnz = -std::numeric_limits<double>::infinity();
+    dlnz[0] = dlnz[1] = dlnz[2] = 0.0;
+    return FTLM_OK;
+  }
+  double zs = 0.0, d[3] = {0.0, 0.0, 0.0};
+  for (const auto& c : cg) {
+    if (!c.ok) continue;
+    const double w = std::exp(-bT * c.lmin - mx);
+    zs += w * c.g;
+    for (int q = 0; q < 3; ++q) d[q] -= w * c.m[q];
+  }
+  *lnz = std::log(static_cast<double>(dim)) + mx + std::log(zs / static_cast<double>(used));
+  for (int q = 0; q < 3; ++q) dlnz[q] = d[q] / zs;
+  if (!op_tp) dlnz[2] = 0.0;
+  return FTLM_OK;
+}
+
+// Per-chain log quadrature and energy ratio with a converged eigen-decomposition (host QL), the
+// quadrature the gradient differentiates; same layout as ftlm_gpu_tridiag_quadrature.
+int ftlm_gpu_tridiag_quadrature_exact(const double* alpha, const double* beta, const int* n, int nc, int ld,
+                                      const double* bts, int n_bt, double* logq, double* energy) {
+  if (nc < 0 || ld <= 0 || n_bt < 0 || !alpha || !beta || !n || (n_bt > 0 && (!bts || !logq || !energy)))
+    return fail(FTLM_ERR_INVALID, "bad arguments");
+  std::vector<double> lam, Z;
+  for (int c = 0; c < nc; ++c) {
+    const int nn = n[c];
+    if (nn > ld) return fail(FTLM_ERR_INVALID, "chain length exceeds ld");
+    double* lq = logq + static_cast<size_t>(c) * n_bt;
+    double* eq = energy + static_cast<size_t>(c) * n_bt;
+    if (nn <= 0) {
+      for (int b = 0; b < n_bt; ++b) {
+        lq[b] = -std::numeric_limits<double>::infinity();
+        eq[b] = 0.0;
+      }
+      continue;
+    }
+    lam.assign(static_cast<size_t>(nn), 0.0);
+    Z.assign(static_cast<size_t>(nn) * nn, 0.0);
+    const std::string err = tridiag_eigvec(nn, alpha + static_cast<size_t>(c) * ld, beta + static_cast<size_t>(c) * ld,
+                                           lam.data(), Z.data());
+    if (!err.empty()) return fail(FTLM_ERR_NUMERIC, err);
+    for (int b = 0; b < n_bt; ++b) {
+      const double bT = bts[b];
+      double z = 0.0, ze = 0.0;
+      for (int j = 0; j < nn; ++j) {
+        const double w = Z[static_cast<size_t>(j)] * Z[static_cast<size_t>(j)] * std::exp(-bT * (lam[static_cast<size_t>(j)] - lam[0]));
+        z += w;
+        ze += w * lam[static_cast<size_t>(j)];
+      }
+      lq[b] = -bT * lam[0] + std::log(z);
+      eq[b] = ze / z;
+    }
+  }
+  return FTLM_OK;
+}
+
+// Host-only helper exposed for tests: eigenvalues/eigenvectors of a symmetric tridiagonal.
+int ftlm_gpu_tridiag_eigvec(const double* alpha, const double* beta, int n, double* lam, double* Z) {
+  if (n < 0 || (n > 0 && (!alpha || !lam || !Z || (n > 1 && !beta)))) return fail(FTLM_ERR_INVALID, "bad arguments");
+  const std::string err = tridiag_eigvec(n, alpha, beta, lam, Z);
+  if (!err.empty()) return fail(FTLM_ERR_NUMERIC, err);
+  return FTLM_OK;
+}
+
+// Host-only helper exposed for tests: the Duhamel weight matrix of one tridiagonal.
+int ftlm_gpu_duhamel_weights(const double* alpha, const double* beta, int n, double bT, double* K, double* g,
+                             double* lam_min) {
+  if (n < 0 || (n > 0 && (!alpha || !K || !g || (n > 1 && !beta)))) return fail(FTLM_ERR_INVALID, "bad arguments");
+  const std::string err = duhamel_weights(n, alpha, beta, bT, K, g, lam_min);
+  if (!err.empty()) return fail(FTLM_ERR_NUMERIC, err);
+  return FTLM_OK;
+}
+
+}  // extern "C"
+
