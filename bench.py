@@ -45,14 +45,15 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--sector", type=int, nargs=2, default=None, metavar=("NU", "ND"),
                     help="profile a smaller 4x4 sector instead (for ncu captures); not a bench line")
-    ap.add_argument("--workload", default="hv", choices=["hv", "batched", "sweep-model", "orbit", "grad", "kresolved"],
+    ap.add_argument("--workload", default="hv", choices=["hv", "batched", "sweep-model", "orbit", "grad", "kresolved", "published"],
                     help="hv: the H·v benchmark (the bench line).  Measurement aids (one JSON line each, not "
                          "bench lines): batched = 32-chain complex64 Lanczos steps on one sector; sweep-model = "
                          "per-sector step cost of the plain and batched paths over the full 4x4 sweep (R=32, "
                          "M=100) and the modelled sweep times; orbit = H_K·v of one momentum block; grad = "
                          "forward and backward of the differentiable 4x3 ln Z_GC (R=32, M=80); kresolved = k-resolved "
                          "sector ln Z (16 orbit blocks, R=24, M=100) against the unsymmetrised batched ln Z "
-                         "(R=32, M=100) of the same sector")
+                         "(R=32, M=100) of the same sector; published = the reference's published n(mu) sweeps "
+                         "(beta=20, R=12, M=72) timed on the GPU next to the published CPU times")
     ap.add_argument("--k", type=int, nargs=2, default=(1, 2), metavar=("KX", "KY"), help="orbit workload momentum")
     return ap.parse_args()
 
@@ -513,6 +514,29 @@ def run_kresolved(args):
     return 0
 
 
+def run_published(args):
+    """The reference's published n(mu) workloads (benchmarks/data/n_vs_mu_*_beta20_*.tsv headers:
+    t'=-0.35, U=5.75, V=0.9, beta=20, R=12, M=72, seed 7), same reference start vectors, timed end to end
+    (sector plans, chains, quadrature, grid).  Published times are the reference's single-threaded
+    CPU runs on the authors' macOS machine, as printed in those files."""
+    import numpy as np
+    import ftlm_extended_hubbard_b200 as F
+    published_s = {"2x2": 0.4258, "3x2": 6.83, "4x2": 105.95, "3x3": 530.327, "2x5": 1877.38}
+    rows = []
+    for key, Lx, Ly in [("2x2", 2, 2), ("3x2", 3, 2), ("4x2", 4, 2), ("3x3", 3, 3), ("2x5", 2, 5)]:
+        p = F.HubbardParams(Lx, Ly, 1.0, -0.35, 5.75, 0.9, 0.0, 0.0)
+        mus = np.linspace(-5.0, 20.0, 221)
+        F.grand_canonical_sweep(F.HubbardParams(2, 2, 1.0, -0.35, 5.75, 0.9, 0.0, 0.0), 2, 4, 7, [0.05], mus[:2])
+        t0 = time.perf_counter()
+        F.grand_canonical_sweep(p, 12, 72, 7, [1.0 / 20.0], mus, start="reference")
+        t = time.perf_counter() - t0
+        rows.append({"lattice": key, "gpu_s": t, "published_cpu_s": published_s[key],
+                     "speedup": published_s[key] / t})
+    print(json.dumps({"workload": "published n(mu) sweeps, beta=20, R=12, M=72 (plain complex128, reference "
+                                  "start vectors)", "rows": rows}))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -527,6 +551,8 @@ def main():
         return run_grad(args)
     if args.workload == "kresolved":
         return run_kresolved(args)
+    if args.workload == "published":
+        return run_published(args)
     return run_ours(args)
 
 

@@ -3,7 +3,10 @@
 // kernels of hv.cu / lanczos.cu / quad.cu.  No exception crosses the ABI.  The batched path,
 // the parameter gradient and the momentum blocks are in capi_batched.cu, capi_grad.cu and
 // capi_orbit.cu.
+#include <thread>
+
 #include "capi_internal.hpp"
+#include "chains.cuh"
 
 using namespace ftlm_b200;
 using namespace ftlm_b200::capi;
@@ -624,6 +627,106 @@ int ftlm_gpu_gc_reduce(const double* lnz_s, const double* e_s, const int* N_s, i
   return FTLM_OK;
 }
 
+}  // extern "C"
+
+namespace ftlm_b200 {
+namespace capi {
+
+int64_t g_fused_max_dim = int64_t(1) << 17;
+
+// ftlm_gpu_ftlm_sector for many small sectors at once: every chain of every sector in one
+// chains_lanczos launch (one CTA per chain), then one batched quadrature; per-sector results in
+// lnz_s/e_s rows out_idx[i].  Same start vectors and seeds as the per-sector path.
+int fused_sectors_ftlm(const std::vector<ftlm_sector*>& secs, const std::vector<int>& out_idx, int R, int M,
+                       unsigned seed, int start_mode, const double* bts, int n_bt, double* lnz_s, double* e_s) {
+  if (secs.empty()) return FTLM_OK;
+  if (start_mode != FTLM_START_REFERENCE && start_mode != FTLM_START_PHILOX)
+    return fail(FTLM_ERR_INVALID, "unknown start_mode");
+  const int ns = static_cast<int>(secs.size());
+  const int nc = ns * R;
+  std::vector<DevSector> devs(static_cast<size_t>(ns));
+  std::vector<ChainDesc> cds(static_cast<size_t>(nc));
+  int64_t total = 0;
+  for (int i = 0; i < ns; ++i) {
+    devs[static_cast<size_t>(i)] = secs[static_cast<size_t>(i)]->dev;
+    for (int r = 0; r < R; ++r) {
+      cds[static_cast<size_t>(i) * R + r] = ChainDesc{i, total};
+      total += 3 * secs[static_cast<size_t>(i)]->plan.dim;
+    }
+  }
+  cudaStream_t st = secs[0]->stream;
+  DevBuf d_sec, d_cd, d_scr, d_a, d_b, d_u, d_red;
+  CU_TRY(d_sec.alloc(devs.size() * sizeof(DevSector)));
+  CU_TRY(d_cd.alloc(cds.size() * sizeof(ChainDesc)));
+  CU_TRY(d_scr.alloc(static_cast<size_t>(total) * sizeof(double2)));
+  CU_TRY(d_a.alloc(static_cast<size_t>(nc) * M * sizeof(double)));
+  CU_TRY(d_b.alloc(static_cast<size_t>(nc) * M * sizeof(double)));
+  CU_TRY(d_u.alloc(static_cast<size_t>(nc) * sizeof(int)));
+  CU_TRY(cudaMemcpyAsync(d_sec.p, devs.data(), devs.size() * sizeof(DevSector), cudaMemcpyHostToDevice, st));
+  CU_TRY(cudaMemcpyAsync(d_cd.p, cds.data(), cds.size() * sizeof(ChainDesc), cudaMemcpyHostToDevice, st));
+  CU_TRY(cudaMemsetAsync(d_a.p, 0, static_cast<size_t>(nc) * M * sizeof(double), st));
+  CU_TRY(cudaMemsetAsync(d_b.p, 0, static_cast<size_t>(nc) * M * sizeof(double), st));
+  double2* scr = d_scr.as<double2>();
+  if (start_mode == FTLM_START_REFERENCE) {
+    // host RNG (libstdc++ mt19937 + normal_distribution, as the reference), chains in parallel
+    std::vector<std::complex<double>> host(static_cast<size_t>(total));
+    const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (unsigned w = 0; w < hw; ++w)
+      pool.emplace_back([&, w]() {
+        std::vector<std::complex<double>> q;
+        for (int c = static_cast<int>(w); c < nc; c += static_cast<int>(hw)) {
+          const int i = c / R, r = c % R;
+          reference_start(secs[static_cast<size_t>(i)]->plan.dim, seed + static_cast<unsigned>(r) * 100003u, &q);
+          std::copy(q.begin(), q.end(), host.begin() + cds[static_cast<size_t>(c)].off);
+        }
+      });
+    for (auto& th : pool) th.join();
+    CU_TRY(cudaMemcpyAsync(scr, host.data(), host.size() * sizeof(double2), cudaMemcpyHostToDevice, st));
+    CU_TRY(cudaStreamSynchronize(st));
+  } else {
+    CU_TRY(d_red.alloc(kScratchDoubles * sizeof(double)));
+    for (int c = 0; c < nc; ++c) {
+      const int i = c / R, r = c % R;
+      const int64_t dim = secs[static_cast<size_t>(i)]->plan.dim;
+      double2* q = scr + cds[static_cast<size_t>(c)].off;
+      CU_TRY(lz_philox_start(q, dim, seed + static_cast<unsigned>(r) * 100003u, d_red.as<double>(), st));
+      CU_TRY(lz_normalise_start(q, dim, d_red.as<double>(), st));
+    }
+  }
+  CU_TRY(chains_lanczos(d_sec.as<DevSector>(), d_cd.as<ChainDesc>(), nc, M, scr, d_a.as<double>(), d_b.as<double>(),
+                        d_u.as<int>(), st));
+  std::vector<double> A(static_cast<size_t>(nc) * M), B(static_cast<size_t>(nc) * M);
+  std::vector<int> used(static_cast<size_t>(nc));
+  CU_TRY(cudaMemcpyAsync(A.data(), d_a.p, A.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaMemcpyAsync(B.data(), d_b.p, B.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaMemcpyAsync(used.data(), d_u.p, used.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaStreamSynchronize(st));
+  std::vector<double> lq(static_cast<size_t>(nc) * n_bt), eq(static_cast<size_t>(nc) * n_bt);
+  int rc = ftlm_gpu_tridiag_quadrature(A.data(), B.data(), used.data(), nc, M, bts, n_bt, lq.data(), eq.data());
+  if (rc) return rc;
+  for (int i = 0; i < ns; ++i) {
+    const size_t o = static_cast<size_t>(i) * R;
+    const size_t dst = static_cast<size_t>(out_idx[static_cast<size_t>(i)]) * n_bt;
+    rc = ftlm_gpu_ftlm_combine(lq.data() + o * n_bt, eq.data() + o * n_bt, used.data() + o, R, n_bt,
+                               std::log(static_cast<double>(secs[static_cast<size_t>(i)]->plan.dim)), lnz_s + dst,
+                               e_s + dst);
+    if (rc) return rc;
+  }
+  return FTLM_OK;
+}
+
+}  // namespace capi
+}  // namespace ftlm_b200
+
+extern "C" {
+
+int ftlm_gpu_set_fused_max_dim(long long max_dim) {
+  if (max_dim < 0) return fail(FTLM_ERR_INVALID, "max_dim must be >= 0");
+  g_fused_max_dim = max_dim;
+  return FTLM_OK;
+}
+
 int ftlm_gpu_gc_sweep(const ftlm_params* p, int R, int M, unsigned seed, int start_mode, const double* bts, int n_bt,
                       const double* mus, int n_mu, double* lnz_s, double* e_s, double* lnz_gc, double* n_avg,
                       double* e_avg) {
@@ -632,18 +735,34 @@ int ftlm_gpu_gc_sweep(const ftlm_params* p, int R, int M, unsigned seed, int sta
   if (n <= 0 || n > 32) return fail(FTLM_ERR_INVALID, "FockBasis: require 1 <= n_sites <= 32 (bit packing)");
   const int nsec = (n + 1) * (n + 1);
   std::vector<int> N(static_cast<size_t>(nsec));
+  std::vector<ftlm_sector*> small;  // sectors for the fused small-sector launch
+  std::vector<int> small_idx;
+  auto clear_and = [](std::vector<ftlm_sector*>& v, int rc) {
+    for (ftlm_sector* x : v) ftlm_gpu_sector_destroy(x);
+    v.clear();
+    return rc;
+  };
   for (int nu = 0; nu <= n; ++nu)
     for (int nd = 0; nd <= n; ++nd) {
       const int idx = nu * (n + 1) + nd;  // benchmarks/bench_ftlm_nmu_rect.cpp:62
       N[static_cast<size_t>(idx)] = nu + nd;
       ftlm_sector* s = nullptr;
       int rc = ftlm_gpu_sector_create(p, nu, nd, &s);
-      if (rc) return rc;
+      if (rc) return clear_and(small, rc);
+      if (s->plan.dim >= 2 && s->plan.dim <= g_fused_max_dim && M <= 160) {  // fused below
+        small.push_back(s);
+        small_idx.push_back(idx);
+        continue;
+      }
       rc = ftlm_gpu_ftlm_sector(s, bts, n_bt, R, M, seed, start_mode, lnz_s + static_cast<size_t>(idx) * n_bt,
                                 e_s + static_cast<size_t>(idx) * n_bt);
       ftlm_gpu_sector_destroy(s);
-      if (rc) return rc;
+      if (rc) return clear_and(small, rc);
     }
+  const int rcf = fused_sectors_ftlm(small, small_idx, std::max(1, R), std::max(1, M), seed, start_mode, bts, n_bt,
+                                     lnz_s, e_s);
+  clear_and(small, FTLM_OK);
+  if (rcf) return rcf;
   if (lnz_gc && n_avg && e_avg)
     return ftlm_gpu_gc_reduce(lnz_s, e_s, N.data(), nsec, bts, n_bt, mus, n_mu, n, lnz_gc, n_avg, e_avg);
   return FTLM_OK;

@@ -24,44 +24,8 @@ namespace {
 __global__ void __launch_bounds__(256) hv_generic_kernel(DevSector S, const double2* __restrict__ x,
                                                          double2* __restrict__ y) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  for (int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; idx < S.dim; idx += stride) {
-    const int64_t r = idx / S.Dd;
-    const int64_t c = idx - r * S.Dd;
-    const uint32_t u = S.umask[r];
-    const uint32_t d = S.dmask[c];
-    double2 acc = make_double2(0.0, 0.0);
-    const double2 xv = x[idx];
-    if (!tiny(xv)) {
-      const double dg = diag_value(S, u, d, S.cnt_uu[r], S.cnt_dd[c], S.wpl[r]);
-      acc.x = dg * xv.x;
-      acc.y = dg * xv.y;
-    }
-    // down hops: sources inside row r
-    const double2* xrow = x + r * S.Dd;
-    const int64_t g = c >> 5;
-    const int lane = static_cast<int>(c & 31);
-    const int64_t e_end = S.dn_gptr[g + 1];
-    for (int64_t p = S.dn_gptr[g] + lane; p < e_end; p += 32) {
-      const uint32_t ent = S.dn_ent[p];
-      const int h = static_cast<int>((ent >> 1) & 511u);
-      if (h == S.n_dn_hops) continue;
-      const double2 xs = xrow[ent >> 10];
-      if (tiny(xs)) continue;
-      const uint32_t neg = (ent & 1u) ^ (static_cast<uint32_t>(__popc(u & S.dn_nmask[h])) & 1u);
-      cmac(acc, S.dn_coef[h], xs, neg);
-    }
-    // up hops: sources in other rows, same column
-    const uint32_t q = prefix_parity_shifted(d);
-    const int j_end = S.up_ptr[r + 1];
-    for (int j = S.up_ptr[r]; j < j_end; ++j) {
-      const double2 xs = x[static_cast<int64_t>(S.up_src[j]) * S.Dd + c];
-      if (tiny(xs)) continue;
-      const uint32_t lh = S.up_lohi[j];
-      const uint32_t neg = ((q >> (lh & 255u)) ^ (q >> (lh >> 8))) & 1u;
-      cmac(acc, S.up_coef[j], xs, neg);
-    }
-    y[idx] = acc;
-  }
+  for (int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; idx < S.dim; idx += stride)
+    y[idx] = hv_element(S, x, idx);
 }
 
 constexpr int kRowThreads = 1024;

@@ -191,6 +191,11 @@ int ftlm_gpu_batched_sweep(const ftlm_params* p, int R, int M, unsigned seed, co
                            double* e_avg);
 int ftlm_gpu_batched_release(void);
 
+/* Sectors with 2 <= dim <= max_dim in ftlm_gpu_gc_sweep run as one fused launch (one CTA per chain,
+ * all M steps on the device; same start vectors and recurrence); default 131072, 0 disables.
+ * No reference counterpart (scheduling only). */
+int ftlm_gpu_set_fused_max_dim(long long max_dim);
+
 /* ---- translation-orbit momentum blocks (sectors built from lattice parameters, n_sites <= 16) ----
  * Basis: canonical orbit representatives (smallest packed up<<16|dn) whose fermionic stabiliser sum
  * |A(K)| > 1e-12, ascending packed order (OrbitKBlockBasis::build, src/orbit_k_block_basis.cpp:70-117).

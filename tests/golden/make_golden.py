@@ -64,7 +64,8 @@ def parse_tsv(path):
 def published():
     out = {}
     for key, fn in [("2x2", "n_vs_mu_2x2_beta20_ftlm.tsv"), ("4x2", "n_vs_mu_4x2_beta20_ftlm.tsv"),
-                    ("3x2_nonmom", "n_vs_mu_3x2_beta20_solver_nonmom.tsv")]:
+                    ("3x2_nonmom", "n_vs_mu_3x2_beta20_solver_nonmom.tsv"), ("3x3", "n_vs_mu_3x3_beta20_ftlm.tsv"),
+                    ("2x5", "n_vs_mu_2x5_beta20_ftlm.tsv"), ("3x2_korbit", "n_vs_mu_3x2_beta20_solver_k_orbit.tsv")]:
         mu, n, hdr = parse_tsv(os.path.join(REF_DATA, fn))
         out[f"{key}_mu"] = mu
         out[f"{key}_n"] = n
