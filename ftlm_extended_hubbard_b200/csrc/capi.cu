@@ -650,7 +650,7 @@ int fused_sectors_ftlm(const std::vector<ftlm_sector*>& secs, const std::vector<
   for (int i = 0; i < ns; ++i) {
     devs[static_cast<size_t>(i)] = secs[static_cast<size_t>(i)]->dev;
     for (int r = 0; r < R; ++r) {
-      cds[static_cast<size_t>(i) * R + r] = ChainDesc{i, total};
+      cds[static_cast<size_t>(i) * R + r] = ChainDesc{i, i * R + r, total};
       total += 3 * secs[static_cast<size_t>(i)]->plan.dim;
     }
   }
@@ -663,7 +663,15 @@ int fused_sectors_ftlm(const std::vector<ftlm_sector*>& secs, const std::vector<
   CU_TRY(d_b.alloc(static_cast<size_t>(nc) * M * sizeof(double)));
   CU_TRY(d_u.alloc(static_cast<size_t>(nc) * sizeof(int)));
   CU_TRY(cudaMemcpyAsync(d_sec.p, devs.data(), devs.size() * sizeof(DevSector), cudaMemcpyHostToDevice, st));
-  CU_TRY(cudaMemcpyAsync(d_cd.p, cds.data(), cds.size() * sizeof(ChainDesc), cudaMemcpyHostToDevice, st));
+  // chains of larger sectors first, 1024 threads each; the rest 256 threads each
+  std::vector<ChainDesc> ordered;
+  ordered.reserve(cds.size());
+  for (const auto& c : cds)
+    if (secs[static_cast<size_t>(c.sector)]->plan.dim > 8192) ordered.push_back(c);
+  const int n_wide = static_cast<int>(ordered.size());
+  for (const auto& c : cds)
+    if (secs[static_cast<size_t>(c.sector)]->plan.dim <= 8192) ordered.push_back(c);
+  CU_TRY(cudaMemcpyAsync(d_cd.p, ordered.data(), ordered.size() * sizeof(ChainDesc), cudaMemcpyHostToDevice, st));
   CU_TRY(cudaMemsetAsync(d_a.p, 0, static_cast<size_t>(nc) * M * sizeof(double), st));
   CU_TRY(cudaMemsetAsync(d_b.p, 0, static_cast<size_t>(nc) * M * sizeof(double), st));
   double2* scr = d_scr.as<double2>();
@@ -694,8 +702,28 @@ int fused_sectors_ftlm(const std::vector<ftlm_sector*>& secs, const std::vector<
       CU_TRY(lz_normalise_start(q, dim, d_red.as<double>(), st));
     }
   }
-  CU_TRY(chains_lanczos(d_sec.as<DevSector>(), d_cd.as<ChainDesc>(), nc, M, scr, d_a.as<double>(), d_b.as<double>(),
-                        d_u.as<int>(), st));
+  // the two launches run concurrently: the small chains on a second stream ordered after the copies
+  cudaStream_t st2 = nullptr;
+  cudaEvent_t ready = nullptr, done = nullptr;
+  CU_TRY(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+  cudaError_t ce = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+  if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
+  if (ce == cudaSuccess) ce = cudaEventRecord(ready, st);
+  if (ce == cudaSuccess) ce = cudaStreamWaitEvent(st2, ready, 0);
+  if (ce == cudaSuccess)
+    ce = chains_lanczos(d_sec.as<DevSector>(), d_cd.as<ChainDesc>(), n_wide, M, scr, d_a.as<double>(),
+                        d_b.as<double>(), d_u.as<int>(), true, st);
+  if (ce == cudaSuccess)
+    ce = chains_lanczos(d_sec.as<DevSector>(), d_cd.as<ChainDesc>() + n_wide, nc - n_wide, M, scr, d_a.as<double>(),
+                        d_b.as<double>(), d_u.as<int>(), false, st2);
+  if (ce == cudaSuccess) ce = cudaEventRecord(done, st2);
+  if (ce == cudaSuccess) ce = cudaStreamWaitEvent(st, done, 0);
+  const cudaError_t se = cudaStreamSynchronize(st);
+  if (ready) cudaEventDestroy(ready);
+  if (done) cudaEventDestroy(done);
+  cudaStreamDestroy(st2);
+  CU_TRY(ce);
+  CU_TRY(se);
   std::vector<double> A(static_cast<size_t>(nc) * M), B(static_cast<size_t>(nc) * M);
   std::vector<int> used(static_cast<size_t>(nc));
   CU_TRY(cudaMemcpyAsync(A.data(), d_a.p, A.size() * sizeof(double), cudaMemcpyDeviceToHost, st));

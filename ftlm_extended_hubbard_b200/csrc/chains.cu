@@ -8,10 +8,8 @@ namespace ftlm_b200 {
 
 namespace {
 
-constexpr int kChainThreads = 256;
-
 // Deterministic block sum of NV doubles; every thread receives the totals.
-template <int NV>
+template <int kChainThreads, int NV>
 __device__ __forceinline__ void block_sum(double (&v)[NV], double* sh) {
   const int t = threadIdx.x;
 #pragma unroll
@@ -28,6 +26,7 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* sh) {
   __syncthreads();
 }
 
+template <int kChainThreads>
 __global__ void __launch_bounds__(kChainThreads) chains_kernel(const DevSector* __restrict__ sectors,
                                                                const ChainDesc* __restrict__ chains, int M,
                                                                double2* __restrict__ scratch, double* __restrict__ alpha,
@@ -40,8 +39,8 @@ __global__ void __launch_bounds__(kChainThreads) chains_kernel(const DevSector* 
   double2* q = scratch + cd.off;
   double2* qp = q + dim;
   double2* w = qp + dim;
-  double* al = alpha + static_cast<int64_t>(blockIdx.x) * M;
-  double* be = beta + static_cast<int64_t>(blockIdx.x) * M;
+  double* al = alpha + static_cast<int64_t>(cd.out) * M;
+  double* be = beta + static_cast<int64_t>(cd.out) * M;
   double bprev = 0.0;
   int nused = 0;
   for (int k = 0; k < M; ++k) {
@@ -53,7 +52,7 @@ __global__ void __launch_bounds__(kChainThreads) chains_kernel(const DevSector* 
       zz[0] += a.x * y.x + a.y * y.y;  // conj(q) w
       zz[1] += a.x * y.y - a.y * y.x;
     }
-    block_sum<2>(zz, sh);
+    block_sum<kChainThreads, 2>(zz, sh);
     const double zr = zz[0], zi = zz[1];
     double n2[1] = {0.0};
     for (int64_t i = t; i < dim; i += kChainThreads) {
@@ -69,7 +68,7 @@ __global__ void __launch_bounds__(kChainThreads) chains_kernel(const DevSector* 
       w[i] = v;
       n2[0] += v.x * v.x + v.y * v.y;
     }
-    block_sum<1>(n2, sh);
+    block_sum<kChainThreads, 1>(n2, sh);
     if (t == 0) al[k] = zr;
     nused = k + 1;
     if (n2[0] < 1e-24) break;  // src/lanczos.cpp:187: alpha_k kept, no beta_k
@@ -86,15 +85,18 @@ __global__ void __launch_bounds__(kChainThreads) chains_kernel(const DevSector* 
     q = tmp;
     bprev = b;
   }
-  if (t == 0) used[blockIdx.x] = nused;
+  if (t == 0) used[cd.out] = nused;
 }
 
 }  // namespace
 
 cudaError_t chains_lanczos(const DevSector* sectors, const ChainDesc* chains, int nc, int M, double2* scratch,
-                           double* alpha, double* beta, int* used, cudaStream_t st) {
+                           double* alpha, double* beta, int* used, bool wide, cudaStream_t st) {
   if (nc <= 0) return cudaSuccess;
-  chains_kernel<<<nc, kChainThreads, 0, st>>>(sectors, chains, M, scratch, alpha, beta, used);
+  if (wide)
+    chains_kernel<1024><<<nc, 1024, 0, st>>>(sectors, chains, M, scratch, alpha, beta, used);
+  else
+    chains_kernel<256><<<nc, 256, 0, st>>>(sectors, chains, M, scratch, alpha, beta, used);
   return cudaGetLastError();
 }
 
