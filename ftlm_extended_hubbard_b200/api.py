@@ -384,6 +384,21 @@ class OrbitKBlock:
         return lnz, en
 
 
+def lanczos_sectors(sectors, n_random: int, lanczos_steps: int, seed: int, start: str = "reference"):
+    """The Lanczos chains of several sectors in one launch (one CTA per chain; for small sectors):
+    alpha/beta [len(sectors)*R][M] (zero-padded), used [len(sectors)*R]; chain r of a sector uses
+    seed + r*100003 as Sector.lanczos."""
+    R, M = n_random, lanczos_steps
+    hs = (C.c_void_p * max(1, len(sectors)))(*[sec.handle.value for sec in sectors])
+    A = np.zeros((len(sectors) * R, M))
+    B = np.zeros((len(sectors) * R, M))
+    u = np.zeros(len(sectors) * R, np.int32)
+    if sectors:
+        call("ftlm_gpu_lanczos_sectors", hs, len(sectors), R, M, C.c_uint(seed & 0xFFFFFFFF), START_MODES[start],
+             A.ctypes.data_as(C.c_void_p), B.ctypes.data_as(C.c_void_p), u.ctypes.data_as(C.c_void_p))
+    return A, B, u
+
+
 @dataclass
 class LanczosExtrema:
     min_eval: float = 0.0

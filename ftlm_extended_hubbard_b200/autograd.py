@@ -25,7 +25,7 @@ import torch
 import ctypes as C
 
 from ._lib import call
-from .api import HubbardParams, Sector
+from .api import HubbardParams, Sector, lanczos_sectors
 
 WEIGHT_CUTOFF = 1e-13
 
@@ -39,32 +39,22 @@ class Lattice:
     phi_y: float = 0.0
 
 
-def _chains(s: Sector, R, M, seed, method, start):
-    """alpha/beta [R][M] and steps used of the forward's chains (same seeds as ftlm/batched_ftlm)."""
-    if method == "batched" and s.dim() > 2 * M:
-        return s.batched_lanczos(R, M, seed)
-    st = "philox" if method == "batched" else start
-    A = np.zeros((R, M))
-    B = np.zeros((R, M))
-    used = np.zeros(R, np.int32)
-    for r in range(R):
-        a, b, u = s.lanczos(M, (seed + r * 100003) & 0xFFFFFFFF, start=st)
-        A[r, :a.size] = a
-        B[r, :b.size] = b
-        used[r] = u
-    return A, B, used
+FUSED_MAX_DIM = 1 << 17  # plain method: sectors up to this size run in one fused launch
 
 
-def _sector_lnz(lat: Lattice, U, V, tp, beta, nu, nd, R, M, seed, method, start):
-    s = Sector(HubbardParams(lat.Lx, lat.Ly, lat.t, tp, U, V, lat.phi_x, lat.phi_y), nu, nd)
-    A, B, used = _chains(s, R, M, seed, method, start)
+def _quadrature(A, B, used, beta, dim):
+    """ln Z_s and E_s from chains (converged tridiagonal quadrature, then the sector combine)."""
+    R, M = A.shape
+    A = np.ascontiguousarray(A)
+    B = np.ascontiguousarray(B)
+    used = np.ascontiguousarray(used, np.int32)
     bt = np.array([float(beta)])
     lq = np.zeros((R, 1))
     eq = np.zeros((R, 1))
     call("ftlm_gpu_tridiag_quadrature_exact", _p(A), _p(B), _p(used), R, M, _p(bt), 1, _p(lq), _p(eq))
     lnz = np.zeros(1)
     en = np.zeros(1)
-    call("ftlm_gpu_ftlm_combine", _p(lq), _p(eq), _p(used), R, 1, float(np.log(s.dim())), _p(lnz), _p(en))
+    call("ftlm_gpu_ftlm_combine", _p(lq), _p(eq), _p(used), R, 1, float(np.log(dim)), _p(lnz), _p(en))
     return float(lnz[0]), float(en[0])
 
 
@@ -73,17 +63,62 @@ def _p(a):
 
 
 def sector_table(lat: Lattice, theta, R, M, seed, method="batched", start="reference"):
-    """ln Z_s, E_s, N_s for every sector at theta = (U, V, t', mu, beta)."""
+    """ln Z_s, E_s, N_s for every sector at theta = (U, V, t', mu, beta).  Chains as the forward FTLM
+    calls make them: method "batched" = complex64 32-chain blocks (sectors with dim <= 2M on the
+    complex128 Philox path), "plain" = complex128 with `start`; the small sectors' chains all in one
+    fused launch."""
     U, V, tp, mu, beta = (float(v) for v in theta)
     n = lat.Lx * lat.Ly
-    lnz, en, N = [], [], []
-    for nu in range(n + 1):
-        for nd in range(n + 1):
-            lz, e = _sector_lnz(lat, U, V, tp, beta, nu, nd, R, M, seed, method, start)
-            lnz.append(lz)
-            en.append(e)
-            N.append(nu + nd)
-    return np.array(lnz), np.array(en), np.array(N, dtype=np.float64)
+    p = HubbardParams(lat.Lx, lat.Ly, lat.t, tp, U, V, lat.phi_x, lat.phi_y)
+    keys = [(nu, nd) for nu in range(n + 1) for nd in range(n + 1)]
+    secs = {k: Sector(p, *k) for k in keys}
+    limit = 2 * M if method == "batched" else FUSED_MAX_DIM
+    small = [k for k in keys if secs[k].dim() <= limit]
+    st = "philox" if method == "batched" else start
+    A, B, used = lanczos_sectors([secs[k] for k in small], R, M, seed, start=st)
+    out = {}
+    for i, k in enumerate(small):
+        out[k] = _quadrature(A[i * R:(i + 1) * R], B[i * R:(i + 1) * R], used[i * R:(i + 1) * R], beta,
+                             secs[k].dim())
+    for k in keys:
+        if k in out:
+            continue
+        s = secs[k]
+        if method == "batched":
+            a, b, u = s.batched_lanczos(R, M, seed)
+        else:
+            a, b, u = _plain_chains(s, R, M, seed, st)
+        out[k] = _quadrature(a, b, u, beta, s.dim())
+    for s in secs.values():
+        s.close()
+    lnz = np.array([out[k][0] for k in keys])
+    en = np.array([out[k][1] for k in keys])
+    N = np.array([nu + nd for nu, nd in keys], dtype=np.float64)
+    return lnz, en, N
+
+
+def _plain_chains(s: Sector, R, M, seed, start):
+    A = np.zeros((R, M))
+    B = np.zeros((R, M))
+    used = np.zeros(R, np.int32)
+    for r in range(R):
+        a, b, u = s.lanczos(M, (seed + r * 100003) & 0xFFFFFFFF, start=start)
+        A[r, :a.size] = a
+        B[r, :b.size] = b
+        used[r] = u
+    return A, B, used
+
+
+def _sector_lnz(lat: Lattice, U, V, tp, beta, nu, nd, R, M, seed, method, start):
+    """One sector's ln Z_s, E_s (same chains and quadrature as sector_table)."""
+    s = Sector(HubbardParams(lat.Lx, lat.Ly, lat.t, tp, U, V, lat.phi_x, lat.phi_y), nu, nd)
+    if method == "batched" and s.dim() > 2 * M:
+        a, b, u = s.batched_lanczos(R, M, seed)
+    elif s.dim() <= (2 * M if method == "batched" else FUSED_MAX_DIM):
+        a, b, u = lanczos_sectors([s], R, M, seed, start="philox" if method == "batched" else start)
+    else:
+        a, b, u = _plain_chains(s, R, M, seed, "philox" if method == "batched" else start)
+    return _quadrature(a, b, u, beta, s.dim())
 
 
 def _lse(x):

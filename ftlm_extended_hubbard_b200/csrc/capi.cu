@@ -637,8 +637,8 @@ int64_t g_fused_max_dim = int64_t(1) << 17;
 // ftlm_gpu_ftlm_sector for many small sectors at once: every chain of every sector in one
 // chains_lanczos launch (one CTA per chain), then one batched quadrature; per-sector results in
 // lnz_s/e_s rows out_idx[i].  Same start vectors and seeds as the per-sector path.
-int fused_sectors_ftlm(const std::vector<ftlm_sector*>& secs, const std::vector<int>& out_idx, int R, int M,
-                       unsigned seed, int start_mode, const double* bts, int n_bt, double* lnz_s, double* e_s) {
+int fused_sectors_lanczos(const std::vector<ftlm_sector*>& secs, int R, int M, unsigned seed, int start_mode,
+                          std::vector<double>* Aout, std::vector<double>* Bout, std::vector<int>* Uout) {
   if (secs.empty()) return FTLM_OK;
   if (start_mode != FTLM_START_REFERENCE && start_mode != FTLM_START_PHILOX)
     return fail(FTLM_ERR_INVALID, "unknown start_mode");
@@ -724,12 +724,28 @@ int fused_sectors_ftlm(const std::vector<ftlm_sector*>& secs, const std::vector<
   cudaStreamDestroy(st2);
   CU_TRY(ce);
   CU_TRY(se);
-  std::vector<double> A(static_cast<size_t>(nc) * M), B(static_cast<size_t>(nc) * M);
-  std::vector<int> used(static_cast<size_t>(nc));
+  std::vector<double>& A = *Aout;
+  std::vector<double>& B = *Bout;
+  std::vector<int>& used = *Uout;
+  A.assign(static_cast<size_t>(nc) * M, 0.0);
+  B.assign(static_cast<size_t>(nc) * M, 0.0);
+  used.assign(static_cast<size_t>(nc), 0);
   CU_TRY(cudaMemcpyAsync(A.data(), d_a.p, A.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
   CU_TRY(cudaMemcpyAsync(B.data(), d_b.p, B.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
   CU_TRY(cudaMemcpyAsync(used.data(), d_u.p, used.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
   CU_TRY(cudaStreamSynchronize(st));
+  return FTLM_OK;
+}
+
+int fused_sectors_ftlm(const std::vector<ftlm_sector*>& secs, const std::vector<int>& out_idx, int R, int M,
+                       unsigned seed, int start_mode, const double* bts, int n_bt, double* lnz_s, double* e_s) {
+  if (secs.empty()) return FTLM_OK;
+  const int ns = static_cast<int>(secs.size());
+  const int nc = ns * R;
+  std::vector<double> A, B;
+  std::vector<int> used;
+  int rc0 = fused_sectors_lanczos(secs, R, M, seed, start_mode, &A, &B, &used);
+  if (rc0) return rc0;
   std::vector<double> lq(static_cast<size_t>(nc) * n_bt), eq(static_cast<size_t>(nc) * n_bt);
   int rc = ftlm_gpu_tridiag_quadrature(A.data(), B.data(), used.data(), nc, M, bts, n_bt, lq.data(), eq.data());
   if (rc) return rc;
@@ -748,6 +764,24 @@ int fused_sectors_ftlm(const std::vector<ftlm_sector*>& secs, const std::vector<
 }  // namespace ftlm_b200
 
 extern "C" {
+
+int ftlm_gpu_lanczos_sectors(ftlm_sector* const* secs, int n_sectors, int R, int M, unsigned seed, int start_mode,
+                             double* alpha, double* beta, int* used) {
+  if (!secs || n_sectors < 0 || R <= 0 || M <= 0 || !alpha || !beta || !used) return fail(FTLM_ERR_INVALID, "bad arguments");
+  std::vector<ftlm_sector*> v(secs, secs + n_sectors);
+  for (ftlm_sector* s : v) {
+    const int rc = need_device(s);
+    if (rc) return rc;
+  }
+  std::vector<double> A, B;
+  std::vector<int> u;
+  const int rc = fused_sectors_lanczos(v, R, M, seed, start_mode, &A, &B, &u);
+  if (rc) return rc;
+  std::copy(A.begin(), A.end(), alpha);
+  std::copy(B.begin(), B.end(), beta);
+  std::copy(u.begin(), u.end(), used);
+  return FTLM_OK;
+}
 
 int ftlm_gpu_set_fused_max_dim(long long max_dim) {
   if (max_dim < 0) return fail(FTLM_ERR_INVALID, "max_dim must be >= 0");

@@ -195,6 +195,11 @@ int ftlm_gpu_batched_release(void);
  * all M steps on the device; same start vectors and recurrence); default 131072, 0 disables.
  * No reference counterpart (scheduling only). */
 int ftlm_gpu_set_fused_max_dim(long long max_dim);
+/* The Lanczos chains of several sectors in one launch (one CTA per chain, all M steps on the device):
+ * chain r of sector i uses seed + r*100003 and start_mode as ftlm_gpu_lanczos; alpha/beta
+ * [n_sectors*R][M] (zero-padded), used [n_sectors*R].  Meant for small sectors (one SM per chain). */
+int ftlm_gpu_lanczos_sectors(ftlm_sector* const* secs, int n_sectors, int R, int M, unsigned seed, int start_mode,
+                             double* alpha, double* beta, int* used);
 
 /* ---- translation-orbit momentum blocks (sectors built from lattice parameters, n_sites <= 16) ----
  * Basis: canonical orbit representatives (smallest packed up<<16|dn) whose fermionic stabiliser sum
