@@ -318,3 +318,18 @@ def test_philox_start_deterministic(gpu):
     a3, _, _ = s.lanczos(12, 43, start="philox")
     assert np.array_equal(a1, a2) and np.array_equal(b1, b2)
     assert not np.array_equal(a1, a3)
+
+
+def test_config1_style_lowest_ritz_values_vs_oracle(gpu):
+    """Config 1's check on a 4x4 sector the CPU can run: (3,3), dim 313,600, t=1 t'=-0.25 U=8 V=1
+    phi_x=0.1, reference start vector (seed 7), M=150: the lowest 5 Ritz values of the GPU chain
+    against the oracle's chain (threaded gather, the reference recurrence) within 1e-10 relative."""
+    import oracle as O
+    c = (4, 4, 1.0, -0.25, 8.0, 1.0, 0.1, 0.0, 3, 3)
+    s = sector_of(c)
+    a, b, used = s.lanczos(150, 7)
+    ao, bo, uo = O.OracleSector(*c).lanczos(150, 7, mode=1, nthreads=16)
+    assert used == uo == 150
+    r_gpu = F.ritz_values(a, b[:149], 5)
+    r_cpu = F.ritz_values(ao, bo[:149], 5)
+    assert np.all(np.abs(r_gpu - r_cpu) <= 1e-10 * np.abs(r_cpu)), (r_gpu, r_cpu)
