@@ -333,3 +333,34 @@ def test_config1_style_lowest_ritz_values_vs_oracle(gpu):
     r_gpu = F.ritz_values(a, b[:149], 5)
     r_cpu = F.ritz_values(ao, bo[:149], 5)
     assert np.all(np.abs(r_gpu - r_cpu) <= 1e-10 * np.abs(r_cpu)), (r_gpu, r_cpu)
+
+
+def test_error_paths_of_sweep_gradient_and_orbit_entry_points(gpu):
+    """Bad arguments come back as status codes with a message, never as a crash."""
+    p = F.HubbardParams(3, 2, 1.0, -0.35, 5.75, 0.9)
+    s = F.Sector(p, 2, 2)
+    other = F.Sector(p, 2, 3)
+    d = np.zeros(3)
+    lnz = C.c_double()
+    with pytest.raises(F.FtlmError) as e:  # operator sector of another (N_up, N_dn)
+        _lib.call("ftlm_gpu_grad_sector", s.handle, other.handle, 1.0, 2, 10, 1, 0, 0, C.byref(lnz),
+                  d.ctypes.data_as(C.c_void_p))
+    assert e.value.code == _lib.FTLM_ERR_INVALID
+    with pytest.raises(F.FtlmError) as e:  # unknown method
+        _lib.call("ftlm_gpu_grad_sector", s.handle, None, 1.0, 2, 10, 1, 7, 0, C.byref(lnz),
+                  d.ctypes.data_as(C.c_void_p))
+    assert e.value.code == _lib.FTLM_ERR_INVALID
+    with pytest.raises(F.FtlmError) as e:  # lattice does not match the site count
+        _lib.call("ftlm_gpu_sector_set_lattice", s.handle, 2, 2)
+    assert e.value.code == _lib.FTLM_ERR_INVALID
+    with pytest.raises(ValueError):  # momentum outside the Brillouin zone
+        s.orbit_block(0, 2)
+    with pytest.raises(F.FtlmError) as e:
+        _lib.call("ftlm_gpu_set_fused_max_dim", -1)
+    assert e.value.code == _lib.FTLM_ERR_INVALID
+    with pytest.raises(F.FtlmError) as e:
+        _lib.call("ftlm_gpu_lanczos_sectors", None, 1, 2, 10, 1, 0, None, None, None)
+    assert e.value.code == _lib.FTLM_ERR_INVALID
+    # the library is still usable afterwards
+    lz, _ = s.ftlm(1.0, 2, 10, 1)
+    assert np.isfinite(lz[0])
