@@ -255,6 +255,7 @@ def run_ours(args):
     p = F.HubbardParams(**PARAMS)
     nu, nd = args.sector if args.sector else (NU, ND)
     sec = F.Sector(p, nu, nd)
+    tuned_path, tuned_cols, _ = sec.autotune(3)  # project autotuner: H·v variant for this sector shape
     st = sec.stats()
     dim = sec.dim()
     g = torch.Generator(device="cuda")
@@ -344,7 +345,8 @@ def run_ours(args):
         "config": {"workload": WORKLOAD if not args.sector else f"4x4 sector {tuple(args.sector)} (profiling case)",
                    "vector": "torch.randn complex128, seed 7+rank",
                    "l2": "inputs larger than L2 (2.65 GB per vector); no flush",
-                   "parallelism": f"independent H·v per rank x{ws}"},
+                   "parallelism": f"independent H·v per rank x{ws}",
+                   "hv_variant": {"path": tuned_path, "cols_slab": [256, 128, 512][tuned_cols], "chosen_by": "autotuner"}},
         "gpu_launches": 2 * args.steps,
         "kernels_ms": {"hv_rows": rows_avg, "hv_cols": cols_avg},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",

@@ -88,6 +88,8 @@ SIGNATURES = {
     "ftlm_gpu_batched_sweep": [C.POINTER(FtlmParams), _i, _i, C.c_uint, _vp, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp],
     "ftlm_gpu_batched_release": [],
     "ftlm_gpu_set_fused_max_dim": [_ll],
+    "ftlm_gpu_autotune_apply": [_vp, _i, _vp, _vp, _vp],
+    "ftlm_gpu_set_cols_variant": [_vp, _i],
     "ftlm_gpu_lanczos_sectors": [_vp, _i, _i, _i, C.c_uint, _i, _vp, _vp, _vp],
     "ftlm_gpu_grad_sector": [_vp, _vp, _d, _i, _i, C.c_uint, _i, _i, _vp, _vp],
     "ftlm_gpu_tridiag_eigvec": [_vp, _vp, _i, _vp, _vp],

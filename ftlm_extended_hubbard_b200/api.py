@@ -228,6 +228,13 @@ class Sector(_Handle):
     def set_apply_path(self, path: int):
         call("ftlm_gpu_set_apply_path", self._h, path)
 
+    def autotune(self, reps: int = 3):
+        """Time the H·v variants of this sector shape and keep the fastest: (path, cols_variant, ms per
+        H·v; -1 when the shape's answer was cached)."""
+        pth, var, ms = C.c_int(), C.c_int(), C.c_float()
+        call("ftlm_gpu_autotune_apply", self._h, reps, C.byref(pth), C.byref(var), C.byref(ms))
+        return pth.value, var.value, ms.value
+
     def apply(self, x, y, stream: int = 0):
         """y = H x on device (torch complex128 tensors or pointers)."""
         call("ftlm_gpu_apply", self._h, C.c_void_p(_ptr(x)), C.c_void_p(_ptr(y)), C.c_void_p(stream))

@@ -3,6 +3,7 @@
 // kernels of hv.cu / lanczos.cu / quad.cu.  No exception crosses the ABI.  The batched path,
 // the parameter gradient and the momentum blocks are in capi_batched.cu, capi_grad.cu and
 // capi_orbit.cu.
+#include <map>
 #include <thread>
 
 #include "capi_internal.hpp"
@@ -324,9 +325,11 @@ int ftlm_gpu_apply_profiled(ftlm_sector* s, const double* x, double* y, void* st
   for (auto& e : ev) CU_TRY(cudaEventCreate(&e));
   CU_TRY(cudaEventRecord(ev[0], st));
   if (path == 2) {
-    CU_TRY(hv_launch_pass(s->dev, reinterpret_cast<const double2*>(x), reinterpret_cast<double2*>(y), 0, st));
+    CU_TRY(hv_launch_pass(s->dev, reinterpret_cast<const double2*>(x), reinterpret_cast<double2*>(y), 0, st,
+                          s->cols_variant));
     CU_TRY(cudaEventRecord(ev[1], st));
-    CU_TRY(hv_launch_pass(s->dev, reinterpret_cast<const double2*>(x), reinterpret_cast<double2*>(y), 1, st));
+    CU_TRY(hv_launch_pass(s->dev, reinterpret_cast<const double2*>(x), reinterpret_cast<double2*>(y), 1, st,
+                          s->cols_variant));
   } else {
     CU_TRY(hv_launch(s->dev, reinterpret_cast<const double2*>(x), reinterpret_cast<double2*>(y), path, st));
     CU_TRY(cudaEventRecord(ev[1], st));
@@ -780,6 +783,82 @@ int ftlm_gpu_lanczos_sectors(ftlm_sector* const* secs, int n_sectors, int R, int
   std::copy(A.begin(), A.end(), alpha);
   std::copy(B.begin(), B.end(), beta);
   std::copy(u.begin(), u.end(), used);
+  return FTLM_OK;
+}
+
+int ftlm_gpu_set_cols_variant(ftlm_sector* s, int variant) {
+  if (!s || variant < 0 || variant > 2) return fail(FTLM_ERR_INVALID, "cols variant must be 0, 1 or 2");
+  s->cols_variant = variant;
+  return FTLM_OK;
+}
+
+int ftlm_gpu_autotune_apply(ftlm_sector* s, int reps, int* path, int* cols_variant, float* ms) {
+  int rc = need_device(s);
+  if (rc) return rc;
+  reps = std::max(1, reps);
+  const SectorPlan& P = s->plan;
+  // one timing per sector shape and process
+  static std::mutex mu;
+  static std::map<std::string, std::pair<int, int>> cache;
+  char key[160];
+  std::snprintf(key, sizeof(key), "%d/%d/%d/%zu/%zu/%d/%d", P.n, P.nu, P.nd, P.hu.size(), P.hd.size(), P.max_up_deg,
+                P.max_dn_deg);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+      s->apply_path = it->second.first;
+      s->cols_variant = it->second.second;
+      if (path) *path = s->apply_path;
+      if (cols_variant) *cols_variant = s->cols_variant;
+      if (ms) *ms = -1.0f;
+      return FTLM_OK;
+    }
+  }
+  const int64_t dim = P.dim;
+  DevBuf x, y;
+  CU_TRY(x.alloc(static_cast<size_t>(dim) * sizeof(double2)));
+  CU_TRY(y.alloc(static_cast<size_t>(dim) * sizeof(double2)));
+  cudaStream_t st = s->stream;
+  CU_TRY(cudaMemsetAsync(x.p, 0, static_cast<size_t>(dim) * sizeof(double2), st));
+  const double one[2] = {1.0, 0.0};
+  CU_TRY(cudaMemcpyAsync(x.p, one, sizeof(double2), cudaMemcpyHostToDevice, st));
+  cudaEvent_t e0, e1;
+  CU_TRY(cudaEventCreate(&e0));
+  CU_TRY(cudaEventCreate(&e1));
+  int best_p = 1, best_v = 0;
+  float best = 3.4e38f;
+  const bool fast = hv_fast_path_ok(s->dev, P.max_up_deg) && hv_rows_smem_bytes(s->dev) <= 227 * 1024;
+  const int variants[4][2] = {{1, 0}, {2, 0}, {2, 1}, {2, 2}};
+  cudaError_t ce = cudaSuccess;
+  for (const auto& v : variants) {
+    if (v[0] == 2 && !fast) continue;
+    ce = hv_launch(s->dev, x.as<double2>(), y.as<double2>(), v[0], st, v[1]);  // warm-up
+    if (ce == cudaSuccess) ce = cudaEventRecord(e0, st);
+    for (int r = 0; r < reps && ce == cudaSuccess; ++r) ce = hv_launch(s->dev, x.as<double2>(), y.as<double2>(), v[0], st, v[1]);
+    if (ce == cudaSuccess) ce = cudaEventRecord(e1, st);
+    if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+    float t = 0.0f;
+    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&t, e0, e1);
+    if (ce != cudaSuccess) break;
+    if (t < best) {
+      best = t;
+      best_p = v[0];
+      best_v = v[1];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CU_TRY(ce);
+  s->apply_path = best_p;
+  s->cols_variant = best_v;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    cache[key] = {best_p, best_v};
+  }
+  if (path) *path = best_p;
+  if (cols_variant) *cols_variant = best_v;
+  if (ms) *ms = best / static_cast<float>(reps);
   return FTLM_OK;
 }
 

@@ -152,7 +152,8 @@ struct ftlm_sector {
   int device = -1;
   ftlm_b200::DevSector dev{};
   std::vector<void*> owned;
-  int apply_path = 0;  // 0 auto, 1 generic, 2 rows+cols
+  int apply_path = 0;    // 0 auto, 1 generic, 2 rows+cols
+  int cols_variant = 0;  // column-slab width of path 2 (hv_launch)
   ftlm_b200::capi::LanczosWs ws;
   ftlm_b200::capi::DevBuf hx, hy;  // staging for the host-buffer apply
   cudaStream_t stream = nullptr;
@@ -168,7 +169,7 @@ struct ftlm_sector {
     const int path = effective_path();
     if (path == 2 && ftlm_b200::hv_rows_smem_bytes(dev) > 227 * 1024)
       return ftlm_b200::capi::fail(FTLM_ERR_UNSUPPORTED, "row pass does not fit in shared memory for this sector");
-    CU_TRY(ftlm_b200::hv_launch(dev, x, y, path, st));
+    CU_TRY(ftlm_b200::hv_launch(dev, x, y, path, st, cols_variant));
     return FTLM_OK;
   }
 };

@@ -91,8 +91,8 @@ __global__ void __launch_bounds__(kRowThreads, 1) hv_rows_kernel(DevSector S, co
   }
 }
 
-constexpr int kColThreads = 128;           // two columns per thread: chunk = 256 columns
-constexpr int kColChunk = 2 * kColThreads;
+// Column pass: two columns per thread, chunk = 2 * threads columns (variants: 64 / 128 / 256
+// threads = 128 / 256 / 512-column slabs of Du * chunk * 16 bytes kept in L2; the autotuner picks).
 constexpr int kMaxUpDeg = 128;
 
 // acc += (-1)^neg c v, the sign applied to c's sign bits.
@@ -106,7 +106,7 @@ __device__ __forceinline__ void cmac_xor(double2& acc, double2 c, double2 v, uin
   acc.y = fma(c.y, v.x, acc.y);
 }
 
-template <bool kFilter>
+template <int kColThreads, bool kFilter>
 __device__ __forceinline__ void cols_body(const DevSector& S, const double2* __restrict__ x, double2* __restrict__ y,
                                           int64_t r, int64_t c0, int deg, const int64_t* s_off, const double2* s_coef,
                                           const uint32_t* s_lh) {
@@ -151,8 +151,10 @@ __device__ __forceinline__ void cols_body(const DevSector& S, const double2* __r
   if (has1) y[r * S.Dd + c1] = acc1;
 }
 
+template <int kColThreads>
 __global__ void __launch_bounds__(kColThreads) hv_cols_kernel(DevSector S, const double2* __restrict__ x,
                                                               double2* __restrict__ y) {
+  constexpr int kColChunk = 2 * kColThreads;
   __shared__ int64_t s_off[kMaxUpDeg];
   __shared__ double2 s_coef[kMaxUpDeg];
   __shared__ uint32_t s_lh[kMaxUpDeg];
@@ -171,9 +173,9 @@ __global__ void __launch_bounds__(kColThreads) hv_cols_kernel(DevSector S, const
   const int64_t c0 = chunk * kColChunk + threadIdx.x;
   if (c0 >= S.Dd) return;
   if (filt)
-    cols_body<true>(S, x, y, r, c0, deg, s_off, s_coef, s_lh);
+    cols_body<kColThreads, true>(S, x, y, r, c0, deg, s_off, s_coef, s_lh);
   else
-    cols_body<false>(S, x, y, r, c0, deg, s_off, s_coef, s_lh);
+    cols_body<kColThreads, false>(S, x, y, r, c0, deg, s_off, s_coef, s_lh);
 }
 
 int g_num_sms = 0;
@@ -197,7 +199,15 @@ void init_sm_count() {
   }
 }
 
-cudaError_t hv_launch_pass(const DevSector& S, const double2* x, double2* y, int pass, cudaStream_t st) {
+template <int kThreads>
+cudaError_t launch_cols(const DevSector& S, const double2* x, double2* y, cudaStream_t st) {
+  const int64_t nchunks = (S.Dd + 2 * kThreads - 1) / (2 * kThreads);
+  hv_cols_kernel<kThreads><<<static_cast<unsigned>(nchunks * S.Du), kThreads, 0, st>>>(S, x, y);
+  return cudaGetLastError();
+}
+
+cudaError_t hv_launch_pass(const DevSector& S, const double2* x, double2* y, int pass, cudaStream_t st,
+                           int cols_variant) {
   if (S.dim <= 0) return cudaSuccess;
   init_sm_count();
   if (pass == 0) {
@@ -210,19 +220,18 @@ cudaError_t hv_launch_pass(const DevSector& S, const double2* x, double2* y, int
     hv_rows_kernel<<<grid_r, kRowThreads, sm, st>>>(S, x, y);
     return cudaGetLastError();
   }
-  const int64_t nchunks = (S.Dd + kColChunk - 1) / kColChunk;
-  const int64_t grid_c = nchunks * S.Du;
-  hv_cols_kernel<<<static_cast<unsigned>(grid_c), kColThreads, 0, st>>>(S, x, y);
-  return cudaGetLastError();
+  if (cols_variant == 1) return launch_cols<64>(S, x, y, st);
+  if (cols_variant == 2) return launch_cols<256>(S, x, y, st);
+  return launch_cols<128>(S, x, y, st);
 }
 
-cudaError_t hv_launch(const DevSector& S, const double2* x, double2* y, int path, cudaStream_t st) {
+cudaError_t hv_launch(const DevSector& S, const double2* x, double2* y, int path, cudaStream_t st, int cols_variant) {
   if (S.dim <= 0) return cudaSuccess;
   init_sm_count();
   if (path == 2) {
-    cudaError_t e = hv_launch_pass(S, x, y, 0, st);
+    cudaError_t e = hv_launch_pass(S, x, y, 0, st, cols_variant);
     if (e != cudaSuccess) return e;
-    return hv_launch_pass(S, x, y, 1, st);
+    return hv_launch_pass(S, x, y, 1, st, cols_variant);
   }
   const int64_t blocks = std::min<int64_t>((S.dim + 255) / 256, static_cast<int64_t>(g_num_sms) * 16);
   hv_generic_kernel<<<static_cast<unsigned>(blocks), 256, 0, st>>>(S, x, y);

@@ -7,10 +7,13 @@
 
 namespace ftlm_b200 {
 
-// path: 1 = generic gather kernel, 2 = row pass + column-slab pass.
-cudaError_t hv_launch(const DevSector& S, const double2* x, double2* y, int path, cudaStream_t st);
+// path: 1 = generic gather kernel, 2 = row pass + column-slab pass.  cols_variant: column slab of
+// 256 (0), 128 (1) or 512 (2) columns.
+cudaError_t hv_launch(const DevSector& S, const double2* x, double2* y, int path, cudaStream_t st,
+                      int cols_variant = 0);
 // One pass of the fast path: 0 = row pass (diag + down hops), 1 = column-slab pass (up hops).
-cudaError_t hv_launch_pass(const DevSector& S, const double2* x, double2* y, int pass, cudaStream_t st);
+cudaError_t hv_launch_pass(const DevSector& S, const double2* x, double2* y, int pass, cudaStream_t st,
+                           int cols_variant = 0);
 bool hv_fast_path_ok(const DevSector& S, int max_up_deg);
 size_t hv_rows_smem_bytes(const DevSector& S);
 

@@ -364,3 +364,32 @@ def test_error_paths_of_sweep_gradient_and_orbit_entry_points(gpu):
     # the library is still usable afterwards
     lz, _ = s.ftlm(1.0, 2, 10, 1)
     assert np.isfinite(lz[0])
+
+
+def test_autotuner_variants_agree(gpu):
+    """Every H·v variant the autotuner chooses from gives the same vector: the column-slab widths
+    bitwise (same terms, same order per element), the generic kernel within rounding."""
+    torch = gpu
+    s = F.Sector(F.HubbardParams(4, 4, 1.0, -0.25, 8.0, 1.0, 0.1, 0.0), 4, 3)
+    x = torch.randn(s.dim(), dtype=torch.complex128, device="cuda")
+    outs = []
+    for v in (0, 1, 2):
+        s.set_apply_path(2)
+        _lib.call("ftlm_gpu_set_cols_variant", s.handle, v)
+        y = torch.empty_like(x)
+        s.apply(x, y)
+        outs.append(y)
+    s.set_apply_path(1)
+    yg = torch.empty_like(x)
+    s.apply(x, yg)
+    torch.cuda.synchronize()
+    assert torch.equal(outs[0], outs[1]) and torch.equal(outs[0], outs[2])
+    assert (outs[0] - yg).abs().max().item() <= RTOL_HV * yg.abs().max().item()
+    p, v, ms = s.autotune(2)
+    assert p in (1, 2) and v in (0, 1, 2) and ms > 0
+    y2 = torch.empty_like(x)
+    s.apply(x, y2)
+    torch.cuda.synchronize()
+    assert (y2 - yg).abs().max().item() <= RTOL_HV * yg.abs().max().item()
+    s2 = F.Sector(F.HubbardParams(4, 4, 1.0, -0.25, 8.0, 1.0, 0.1, 0.0), 4, 3)
+    assert s2.autotune(2) == (p, v, -1.0)  # cached per sector shape
