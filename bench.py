@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--sector", type=int, nargs=2, default=None, metavar=("NU", "ND"),
                     help="profile a smaller 4x4 sector instead (for ncu captures); not a bench line")
-    ap.add_argument("--workload", default="hv", choices=["hv", "batched", "sweep-model", "orbit", "grad", "kresolved", "published"],
+    ap.add_argument("--workload", default="hv", choices=["hv", "batched", "sweep-model", "orbit", "grad", "kresolved", "published", "sweep"],
                     help="hv: the H·v benchmark (the bench line).  Measurement aids (one JSON line each, not "
                          "bench lines): batched = 32-chain complex64 Lanczos steps on one sector; sweep-model = "
                          "per-sector step cost of the plain and batched paths over the full 4x4 sweep (R=32, "
@@ -53,7 +53,9 @@ def parse():
                          "forward and backward of the differentiable 4x3 ln Z_GC (R=32, M=80); kresolved = k-resolved "
                          "sector ln Z (16 orbit blocks, R=24, M=100) against the unsymmetrised batched ln Z "
                          "(R=32, M=100) of the same sector; published = the reference's published n(mu) sweeps "
-                         "(beta=20, R=12, M=72) timed on the GPU next to the published CPU times")
+                         "(beta=20, R=12, M=72) timed on the GPU next to the published CPU times; sweep = the full 4x4 "
+                         "grand-canonical sweep, batched complex64 and plain complex128 (same Philox starts), "
+                         "R=32, M=100, T=0.1..2 x mu=-4..8 (tens of minutes)")
     ap.add_argument("--k", type=int, nargs=2, default=(1, 2), metavar=("KX", "KY"), help="orbit workload momentum")
     return ap.parse_args()
 
@@ -556,6 +558,32 @@ def run_published(args):
     return 0
 
 
+def run_sweep(args):
+    """The full 4x4 sweep (289 sectors, R=32, M=100) with both paths, end to end, and the batched
+    path's errors against complex128 with the same Philox start vectors."""
+    import numpy as np
+    import ftlm_extended_hubbard_b200 as F
+    p = F.HubbardParams(**PARAMS)
+    T = np.round(np.arange(1, 21) * 0.1, 10)
+    mu = np.round(np.arange(49) * 0.25 - 4.0, 10)
+    t0 = time.perf_counter()
+    rb = F.grand_canonical_sweep(p, 32, 100, 7, T, mu, method="batched")
+    tb = time.perf_counter() - t0
+    F.batched_release()
+    t0 = time.perf_counter()
+    rp = F.grand_canonical_sweep(p, 32, 100, 7, T, mu, start="philox")
+    tp = time.perf_counter() - t0
+    ok = np.isfinite(rp.lnz_sector)
+    rel_s = np.abs(rb.lnz_sector[ok] - rp.lnz_sector[ok]) / np.maximum(1.0, np.abs(rp.lnz_sector[ok]))
+    rel_g = np.abs(rb.lnz_gc - rp.lnz_gc) / np.maximum(1.0, np.abs(rp.lnz_gc))
+    print(json.dumps({"workload": "full 4x4 grand-canonical sweep, 289 sectors, R=32, M=100, T 0.1..2 (20) x mu "
+                                  "-4..8 (49), t=1 t'=-0.25 U=8 V=1 phi_x=0.1",
+                      "batched_s": tb, "plain_s": tp, "ratio": tp / tb,
+                      "max_rel_err_sector_lnz": float(rel_s.max()), "max_rel_err_gc_lnz": float(rel_g.max()),
+                      "max_abs_err_n": float(np.abs(rb.n_avg - rp.n_avg).max())}))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -572,6 +600,8 @@ def main():
         return run_kresolved(args)
     if args.workload == "published":
         return run_published(args)
+    if args.workload == "sweep":
+        return run_sweep(args)
     return run_ours(args)
 
 
