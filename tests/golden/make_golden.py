@@ -13,7 +13,7 @@ published_korbit.npz  the reference's published k-orbit run on 3x2 (benchmarks/d
 orbit_small.npz    translation-orbit momentum blocks from the reference library (OrbitKBlockBasis::build,
                    apply_orbit_k_block, ftlm_log_partition_complex): representatives, |A|, orbit sizes,
                    H_K x on seeded vectors and block ln Z.
-config0_4x2.npz    the plain FTLM sweep of 4x2, t=1 t'=-0.25 U=8 V=1, phi=0, R=20, M=60, seed 7,
+sweep_4x2.npz    the plain FTLM sweep of 4x2, t=1 t'=-0.25 U=8 V=1, phi=0, R=20, M=60, seed 7,
                    T = 0.1..2.0 (20) x mu = -4..8 (49), computed by the oracle in the reference's
                    scatter order (bit-identical to the reference library; this script checks the
                    sector ln Z of several sectors against the reference itself before writing).
@@ -183,13 +183,13 @@ def orbit_small():
     return out
 
 
-CONFIG0 = dict(Lx=4, Ly=2, t=1.0, tp=-0.25, U=8.0, V=1.0, phix=0.0, phiy=0.0, R=20, M=60, seed=7)
+SWEEP_4X2 = dict(Lx=4, Ly=2, t=1.0, tp=-0.25, U=8.0, V=1.0, phix=0.0, phiy=0.0, R=20, M=60, seed=7)
 T_GRID = np.round(np.arange(1, 21) * 0.1, 10)
 MU_GRID = np.round(np.arange(49) * 0.25 - 4.0, 10)
 
 
-def config0():
-    c = CONFIG0
+def sweep_4x2():
+    c = SWEEP_4X2
     betas = 1.0 / T_GRID
     lz, es, N, dims, (g_lnz, g_n, g_e) = O.oracle_sweep(c["Lx"], c["Ly"], c["t"], c["tp"], c["U"], c["V"], c["phix"],
                                                        c["phiy"], c["R"], c["M"], c["seed"], betas, MU_GRID, mode=0)
@@ -215,7 +215,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "ref_small.npz"), **ref_small())
     np.savez_compressed(os.path.join(HERE, "orbit_small.npz"), **orbit_small())
     np.savez_compressed(os.path.join(HERE, "published_korbit.npz"), **published_korbit())
-    np.savez_compressed(os.path.join(HERE, "config0_4x2.npz"), **config0())
+    np.savez_compressed(os.path.join(HERE, "sweep_4x2.npz"), **sweep_4x2())
     print("wrote", os.listdir(HERE))
 
 

@@ -29,8 +29,8 @@ def test_fused_sweep_matches_per_sector_path(gpu, start):
     assert np.abs(r1.n_avg - r0.n_avg).max() <= 1e-12
 
 
-def test_fused_sweep_reproduces_config0_golden(gpu, golden):
-    g = golden("config0_4x2.npz")
+def test_fused_sweep_reproduces_4x2_golden(gpu, golden):
+    g = golden("sweep_4x2.npz")
     Lx, Ly, t, tp, U, V, px, py, R, M, seed = g["params"]
     p = F.HubbardParams(int(Lx), int(Ly), t, tp, U, V, px, py)
     r = F.grand_canonical_sweep(p, int(R), int(M), int(seed), g["T"], g["mu"], start="reference")

@@ -211,9 +211,9 @@ def test_lanczos_extrema_matches_reference(gpu, golden):
         assert r.min() - tol <= e.min_eval <= e.max_eval <= r.max() + tol
 
 
-def test_config0_plain_sweep_matches_golden(gpu, golden):
+def test_plain_sweep_4x2_matches_golden(gpu, golden):
     """4x2, t'=-0.25, U=8, V=1: all 81 sectors, R=20, M=60, seed 7; ln Z, <n>, <E> on 20 T x 49 mu."""
-    g = golden("config0_4x2.npz")
+    g = golden("sweep_4x2.npz")
     p = F.HubbardParams(4, 2, 1.0, -0.25, 8.0, 1.0, 0.0, 0.0)
     r = F.grand_canonical_sweep(p, 20, 60, 7, g["T"], g["mu"])
     assert relerr(r.lnz_sector, g["lnz_sector"]) < RTOL_THERMO
@@ -320,8 +320,8 @@ def test_philox_start_deterministic(gpu):
     assert not np.array_equal(a1, a3)
 
 
-def test_config1_style_lowest_ritz_values_vs_oracle(gpu):
-    """Config 1's check on a 4x4 sector the CPU can run: (3,3), dim 313,600, t=1 t'=-0.25 U=8 V=1
+def test_lowest_ritz_values_4x4_vs_oracle(gpu):
+    """The 4x4 Ritz-value check on a sector the CPU can run: (3,3), dim 313,600, t=1 t'=-0.25 U=8 V=1
     phi_x=0.1, reference start vector (seed 7), M=150: the lowest 5 Ritz values of the GPU chain
     against the oracle's chain (threaded gather, the reference recurrence) within 1e-10 relative."""
     import oracle as O

@@ -146,8 +146,8 @@ def test_oracle_reproduces_published_tsv(golden, key, Lx, Ly):
             assert abs(lz[nu * 7 + nd] - lzp) <= 5e-6 * max(1.0, abs(lzp))
 
 
-def test_config0_golden_is_self_consistent(golden):
-    g = golden("config0_4x2.npz")
+def test_sweep_4x2_golden_is_self_consistent(golden):
+    g = golden("sweep_4x2.npz")
     lz = g["lnz_sector"]
     assert lz.shape == (81, 20)
     assert np.isfinite(lz).all()
