@@ -76,18 +76,35 @@ int ftlm_gpu_batched_sweep(const ftlm_params* p, int R, int M, unsigned seed, co
   if (n <= 0 || n > 32) return fail(FTLM_ERR_INVALID, "FockBasis: require 1 <= n_sites <= 32 (bit packing)");
   const int nsec = (n + 1) * (n + 1);
   std::vector<int> N(static_cast<size_t>(nsec));
+  // sectors the batched path runs in complex128 (dim <= 2M, Philox starts) go to one fused launch
+  std::vector<ftlm_sector*> small;
+  std::vector<int> small_idx;
+  auto clear_and = [&small](int rc) {
+    for (ftlm_sector* x : small) ftlm_gpu_sector_destroy(x);
+    small.clear();
+    return rc;
+  };
   for (int nu = 0; nu <= n; ++nu)
     for (int nd = 0; nd <= n; ++nd) {
       const int idx = nu * (n + 1) + nd;
       N[static_cast<size_t>(idx)] = nu + nd;
       ftlm_sector* s = nullptr;
       int rc = ftlm_gpu_sector_create(p, nu, nd, &s);
-      if (rc) return rc;
+      if (rc) return clear_and(rc);
+      if (s->plan.dim >= 2 && s->plan.dim <= 2 * static_cast<int64_t>(std::max(1, M)) && M <= 160) {
+        small.push_back(s);
+        small_idx.push_back(idx);
+        continue;
+      }
       rc = ftlm_gpu_batched_ftlm_sector(s, bts, n_bt, R, M, seed, lnz_s + static_cast<size_t>(idx) * n_bt,
                                         e_s + static_cast<size_t>(idx) * n_bt);
       ftlm_gpu_sector_destroy(s);
-      if (rc) return rc;
+      if (rc) return clear_and(rc);
     }
+  const int rcf = fused_sectors_ftlm(small, small_idx, std::max(1, R), std::max(1, M), seed, FTLM_START_PHILOX, bts,
+                                     n_bt, lnz_s, e_s);
+  clear_and(FTLM_OK);
+  if (rcf) return rcf;
   if (lnz_gc && n_avg && e_avg)
     return ftlm_gpu_gc_reduce(lnz_s, e_s, N.data(), nsec, bts, n_bt, mus, n_mu, n, lnz_gc, n_avg, e_avg);
   return FTLM_OK;

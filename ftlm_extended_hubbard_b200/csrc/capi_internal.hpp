@@ -297,6 +297,11 @@ int bt_run_chains_impl(int64_t dim, cudaStream_t st, Step&& step, int R, int M, 
   return FTLM_OK;
 }
 
+// ftlm_gpu_ftlm_sector for many small sectors in one chains_lanczos launch (capi.cu); results in
+// rows out_idx[i] of lnz_s / e_s.
+int fused_sectors_ftlm(const std::vector<ftlm_sector*>& secs, const std::vector<int>& out_idx, int R, int M,
+                       unsigned seed, int start_mode, const double* bts, int n_bt, double* lnz_s, double* e_s);
+
 // 32-chain blocks of one sector (bt_step), alpha/beta [R][M], steps used [R].
 int bt_run_chains(ftlm_sector* s, int R, int M, unsigned seed, std::vector<double>* A, std::vector<double>* B,
                   std::vector<int>* used);
