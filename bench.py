@@ -57,7 +57,6 @@ def parse():
                          "grand-canonical sweep, batched complex64 and plain complex128 (same Philox starts), "
                          "R=32, M=100, T=0.1..2 x mu=-4..8 (tens of minutes)")
     ap.add_argument("--k", type=int, nargs=2, default=(1, 2), metavar=("KX", "KY"), help="orbit workload momentum")
-    ap.add_argument("--lattice", default=None, help="published workload: run only this lattice (e.g. 3x3), once")
     return ap.parse_args()
 
 
@@ -528,24 +527,18 @@ def run_published(args):
     import ftlm_extended_hubbard_b200 as F
     published_s = {"2x2": 0.4258, "3x2": 6.83, "4x2": 105.95, "3x3": 530.327, "2x5": 1877.38}
     rows = []
-    todo = [("2x2", 2, 2), ("3x2", 3, 2), ("4x2", 4, 2), ("3x3", 3, 3), ("2x5", 2, 5)]
-    if args.lattice:
-        todo = [t for t in todo if t[0] == args.lattice]
-    for key, Lx, Ly in todo:
+    for key, Lx, Ly in [("2x2", 2, 2), ("3x2", 3, 2), ("4x2", 4, 2), ("3x3", 3, 3), ("2x5", 2, 5)]:
         p = F.HubbardParams(Lx, Ly, 1.0, -0.35, 5.75, 0.9, 0.0, 0.0)
         mus = np.linspace(-5.0, 20.0, 221)
         F.grand_canonical_sweep(F.HubbardParams(2, 2, 1.0, -0.35, 5.75, 0.9, 0.0, 0.0), 2, 4, 7, [0.05], mus[:2])
         ts = []
-        for _ in range(1 if args.lattice else 3):  # median of three end-to-end runs
+        for _ in range(3):  # median of three end-to-end runs
             t0 = time.perf_counter()
             F.grand_canonical_sweep(p, 12, 72, 7, [1.0 / 20.0], mus, start="reference")
             ts.append(time.perf_counter() - t0)
-        t = sorted(ts)[len(ts) // 2]
+        t = sorted(ts)[1]
         rows.append({"lattice": key, "gpu_s": t, "published_cpu_s": published_s[key],
                      "speedup": published_s[key] / t})
-    if args.lattice:
-        print(json.dumps({"workload": f"published n(mu) sweep {args.lattice}, beta=20, R=12, M=72", "rows": rows}))
-        return 0
     # the k-orbit solver run (3x2, momentum blocks; blocks of dim <= 64 exactly, larger by FTLM)
     p = F.HubbardParams(3, 2, 1.0, -0.35, 5.75, 0.9, 0.0, 0.0)
     ts = []

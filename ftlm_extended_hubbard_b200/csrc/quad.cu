@@ -61,65 +61,59 @@ __global__ void __launch_bounds__(kJacThreads) jacobi_kernel(const double* __res
   }
   for (int i = tid; i < n; i += kJacThreads) v0[i] = (i == 0) ? 1.0 : 0.0;
   __syncthreads();
-  // Pivot search without rescanning the matrix: per row i the largest |A_ij| over j > i (first such j)
-  // is kept in rmax/ridx and updated after each rotation, which changes only rows/columns p and q.
-  // The global pivot is the first row with the largest row maximum: the same element as the
-  // reference's row-major scan with a strict '>', so the rotation sequence is unchanged.
-  double* rmax = v0 + n;
-  int* ridx = reinterpret_cast<int*>(rmax + n);
-  auto row_scan = [&](int r) {
-    double best = -1.0;
-    int bi = -1;
-    for (int c = r + 1; c < n; ++c) {
-      const double v = fabs(A[r * n + c]);
-      if (v > best) {
-        best = v;
-        bi = c;
-      }
-    }
-    rmax[r] = best;
-    ridx[r] = bi;
-  };
-  for (int r = tid; r < n; r += kJacThreads) row_scan(r);
-  __syncthreads();
   const int max_rot = max_rot_in > 0 ? max_rot_in : max(3000, 120 * n);
   const int lane = tid & 31, warp = tid >> 5;
   for (int rot = 0; rot < max_rot; ++rot) {
-    if (warp == 0) {
-      double best = -1.0;
-      int brow = 0x7fffffff;
-      for (int r = lane; r < n; r += 32) {
-        const double v = rmax[r];
-        if (v > best) {
-          best = v;
-          brow = r;
-        }
+    // Pivot: largest |A_ij| over i<j, first in row-major order (strict > as the reference).
+    double best = 0.0;
+    int bidx = 0x7fffffff;
+    for (int L = tid; L < n * n; L += kJacThreads) {
+      const int r = L / n, c = L - r * n;
+      if (c <= r) continue;
+      const double v = fabs(A[L]);
+      if (v > best) {
+        best = v;
+        bidx = L;
       }
+    }
 #pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const double ov = __shfl_down_sync(0xffffffffu, best, off);
-        const int orow = __shfl_down_sync(0xffffffffu, brow, off);
-        if (ov > best || (ov == best && orow < brow)) {
-          best = ov;
-          brow = orow;
-        }
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ov = __shfl_down_sync(0xffffffffu, best, off);
+      const int oi = __shfl_down_sync(0xffffffffu, bidx, off);
+      if (ov > best || (ov == best && oi < bidx)) {
+        best = ov;
+        bidx = oi;
       }
-      if (lane == 0) {
-        // reference: break if max_abs < tol (max_abs starts at 0)
-        const double bv = best < 0.0 ? 0.0 : best;
-        s_stop = !(bv >= tol);
-        if (!s_stop) {
-          const int p = brow, q = ridx[brow];
-          const double app = A[p * n + p], aqq = A[q * n + q], apq = A[p * n + q];
-          const double phi = mul(0.5, atan2(mul(2.0, apq), sub(aqq, app)));
-          s_c = cos(phi);
-          s_s = sin(phi);
-          s_app = app;
-          s_aqq = aqq;
-          s_apq = apq;
-          s_p = p;
-          s_q = q;
+    }
+    if (lane == 0) {
+      red_v[warp] = best;
+      red_i[warp] = bidx;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double bv = red_v[0];
+      int bi = red_i[0];
+      for (int w = 1; w < kJacThreads / 32; ++w)
+        if (red_v[w] > bv || (red_v[w] == bv && red_i[w] < bi)) {
+          bv = red_v[w];
+          bi = red_i[w];
         }
+      int p = 0, q = 1;
+      if (bi != 0x7fffffff) {
+        p = bi / n;
+        q = bi - p * n;
+      }
+      s_stop = !(bv >= tol);  // reference: break if max_abs < tol (max_abs starts at 0)
+      if (!s_stop) {
+        const double app = A[p * n + p], aqq = A[q * n + q], apq = A[p * n + q];
+        const double phi = mul(0.5, atan2(mul(2.0, apq), sub(aqq, app)));
+        s_c = cos(phi);
+        s_s = sin(phi);
+        s_app = app;
+        s_aqq = aqq;
+        s_apq = apq;
+        s_p = p;
+        s_q = q;
       }
     }
     __syncthreads();
@@ -148,31 +142,6 @@ __global__ void __launch_bounds__(kJacThreads) jacobi_kernel(const double* __res
       const double vip = v0[p], viq = v0[q];
       v0[p] = sub(mul(c, vip), mul(s, viq));
       v0[q] = add(mul(s, vip), mul(c, viq));
-    }
-    __syncthreads();
-    // rows whose upper part changed: p and q entirely; any row k < q in columns p (if k < p) and q
-    for (int k = tid; k < n; k += kJacThreads) {
-      if (k == p || k == q || ridx[k] == p || ridx[k] == q) {
-        if (k == p || k == q || k < q) row_scan(k);
-        continue;
-      }
-      if (k >= q) continue;
-      double best = rmax[k];
-      int bi = ridx[k];
-      if (k < p) {
-        const double v = fabs(A[k * n + p]);
-        if (v > best || (v == best && p < bi)) {
-          best = v;
-          bi = p;
-        }
-      }
-      const double v = fabs(A[k * n + q]);
-      if (v > best || (v == best && q < bi)) {
-        best = v;
-        bi = q;
-      }
-      rmax[k] = best;
-      ridx[k] = bi;
     }
     __syncthreads();
   }
@@ -329,8 +298,7 @@ __global__ void ritz_kernel(const double* __restrict__ a, const double* __restri
 cudaError_t quad_jacobi(const double* alpha, const double* beta, const int* n, int nc, int ld, int max_rot,
                         double tol, double* lam, double* w0, cudaStream_t st) {
   if (nc <= 0) return cudaSuccess;
-  const size_t sm = (static_cast<size_t>(ld) * ld + 2 * static_cast<size_t>(ld)) * sizeof(double) +
-                    static_cast<size_t>(ld) * sizeof(int);
+  const size_t sm = (static_cast<size_t>(ld) * ld + ld) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
   if (e != cudaSuccess) return e;
   jacobi_kernel<<<nc, kJacThreads, sm, st>>>(alpha, beta, n, ld, max_rot, tol, lam, w0);
