@@ -131,6 +131,19 @@ def grand_canonical_logz_value(lat: Lattice, theta, R, M, seed, method="batched"
     return _lse(lnz + float(theta[4]) * float(theta[3]) * N)
 
 
+def gc_combine(lnz, en, N, mu: float, beta: float):
+    """ln Z_GC = log sum_s exp(ln Z_s + beta mu N_s) and the parts of its gradient that need no chain
+    replay: the sector weights w_s, d/dmu = beta <N> and d/dbeta = <mu N - E> (E_s: the FTLM energy
+    of the same quadrature, which is -d ln Z_s / d beta exactly)."""
+    lnz = np.asarray(lnz, dtype=np.float64)
+    x = lnz + beta * mu * np.asarray(N, dtype=np.float64)
+    lnZ = _lse(x)
+    w = np.exp(x - lnZ)
+    dmu = beta * float(np.sum(w * N))
+    dbeta = float(np.sum(w * (mu * np.asarray(N, dtype=np.float64) - np.asarray(en, dtype=np.float64))))
+    return lnZ, w, dmu, dbeta
+
+
 class GrandCanonicalLogZ(torch.autograd.Function):
     """theta: float64 tensor (U, V, t', mu, beta).  Returns the scalar ln Z_GC."""
 
@@ -139,8 +152,7 @@ class GrandCanonicalLogZ(torch.autograd.Function):
                 start: str = "reference"):
         th = theta.detach().cpu().double().numpy()
         lnz, en, N = sector_table(lat, th, R, M, seed, method, start)
-        x = lnz + th[4] * th[3] * N
-        lnZ = _lse(x)
+        lnZ = gc_combine(lnz, en, N, th[3], th[4])[0]
         ctx.save_for_backward(theta)
         ctx.cfg = (lat, R, M, seed, method, start)
         ctx.table = (lnz, en, N, lnZ)
@@ -152,7 +164,7 @@ class GrandCanonicalLogZ(torch.autograd.Function):
         lat, R, M, seed, method, start = ctx.cfg
         lnz, en, N, lnZ = ctx.table
         U, V, tp, mu, beta = (float(v) for v in theta.detach().cpu().double().numpy())
-        w = np.exp(lnz + beta * mu * N - lnZ)
+        _, w, dmu, dbeta = gc_combine(lnz, en, N, mu, beta)
         d = np.zeros(3)
         n = lat.Lx * lat.Ly
         k = 0
@@ -170,8 +182,6 @@ class GrandCanonicalLogZ(torch.autograd.Function):
                     raise RuntimeError(f"gradient replay of sector ({nu},{nd}) did not reproduce the forward "
                                        f"ln Z ({lz} vs {lnz[k - 1]})")
                 d += ws * g
-        dmu = beta * float(np.sum(w * N))
-        dbeta = float(np.sum(w * (mu * N - en)))
         grad = theta.new_tensor([d[0], d[1], d[2], dmu, dbeta])
         return grad_out * grad, None, None, None, None, None, None
 
