@@ -92,6 +92,8 @@ SIGNATURES = {
     "ftlm_gpu_set_cols_variant": [_vp, _i],
     "ftlm_gpu_lanczos_sectors": [_vp, _i, _i, _i, C.c_uint, _i, _vp, _vp, _vp],
     "ftlm_gpu_grad_sector": [_vp, _vp, _d, _i, _i, C.c_uint, _i, _i, _vp, _vp],
+    "ftlm_gpu_gc_logz": [C.POINTER(FtlmParams), _d, _d, _i, _i, C.c_uint, _i, _i, _vp, _vp, _pd],
+    "ftlm_gpu_gc_logz_grad": [C.POINTER(FtlmParams), _d, _d, _i, _i, C.c_uint, _i, _i, _vp, _vp, _vp],
     "ftlm_gpu_tridiag_eigvec": [_vp, _vp, _i, _vp, _vp],
     "ftlm_gpu_tridiag_quadrature_exact": [_vp, _vp, _vp, _i, _i, _vp, _i, _vp, _vp],
     "ftlm_gpu_duhamel_weights": [_vp, _vp, _i, _d, _vp, _vp, _vp],

@@ -12,8 +12,9 @@ Backward (the reference has no derivatives):
     d/dbeta = <mu N - E>          (E_s: the FTLM energy of the same quadrature, exact derivative),
     d/dtheta for theta in (U, V, t'): sum_s w_s d ln Z_s/dtheta, w_s = exp(ln Z_s + beta mu N_s - ln Z_GC),
 where d ln Z_s/dtheta re-runs the sector's chains from their seed on the GPU
-(Sector.ftlm_grad: Duhamel derivative in each chain's Krylov space, start vectors fixed).
-Sectors with w_s < 1e-13 are skipped (their term is below 1e-13 * beta * n_sites).
+(ftlm_gpu_grad_sector: Duhamel derivative in each chain's Krylov space, start vectors fixed).
+Sectors with w_s < 1e-13 are skipped (their term is below 1e-13 * beta * n_sites).  The sector loop,
+quadrature and combination run in the native library (ftlm_gpu_gc_logz / ftlm_gpu_gc_logz_grad).
 """
 from __future__ import annotations
 
@@ -24,10 +25,10 @@ import torch
 
 import ctypes as C
 
-from ._lib import call
-from .api import HubbardParams, Sector, lanczos_sectors
+from ._lib import FTLM_START_PHILOX, FTLM_START_REFERENCE, call
+from .api import HubbardParams
 
-WEIGHT_CUTOFF = 1e-13
+START_MODES = {"reference": FTLM_START_REFERENCE, "philox": FTLM_START_PHILOX}
 
 
 @dataclass(frozen=True)
@@ -39,86 +40,45 @@ class Lattice:
     phi_y: float = 0.0
 
 
-FUSED_MAX_DIM = 1 << 17  # plain method: sectors up to this size run in one fused launch
-
-
-def _quadrature(A, B, used, beta, dim):
-    """ln Z_s and E_s from chains (converged tridiagonal quadrature, then the sector combine)."""
-    R, M = A.shape
-    A = np.ascontiguousarray(A)
-    B = np.ascontiguousarray(B)
-    used = np.ascontiguousarray(used, np.int32)
-    bt = np.array([float(beta)])
-    lq = np.zeros((R, 1))
-    eq = np.zeros((R, 1))
-    call("ftlm_gpu_tridiag_quadrature_exact", _p(A), _p(B), _p(used), R, M, _p(bt), 1, _p(lq), _p(eq))
-    lnz = np.zeros(1)
-    en = np.zeros(1)
-    call("ftlm_gpu_ftlm_combine", _p(lq), _p(eq), _p(used), R, 1, float(np.log(dim)), _p(lnz), _p(en))
-    return float(lnz[0]), float(en[0])
+METHODS = {"plain": 0, "batched": 1}
 
 
 def _p(a):
     return a.ctypes.data_as(C.c_void_p)
 
 
+def _params(lat: Lattice, U, V, tp) -> HubbardParams:
+    return HubbardParams(lat.Lx, lat.Ly, lat.t, float(tp), float(U), float(V), lat.phi_x, lat.phi_y)
+
+
 def sector_table(lat: Lattice, theta, R, M, seed, method="batched", start="reference"):
-    """ln Z_s, E_s, N_s for every sector at theta = (U, V, t', mu, beta).  Chains as the forward FTLM
-    calls make them: method "batched" = complex64 32-chain blocks (sectors with dim <= 2M on the
-    complex128 Philox path), "plain" = complex128 with `start`; the small sectors' chains all in one
-    fused launch."""
+    """ln Z_s, E_s, N_s for every sector at theta = (U, V, t', mu, beta), and ln Z_GC (ftlm_gpu_gc_logz).
+    Chains as the forward FTLM calls make them: method "batched" = complex64 32-chain blocks (sectors
+    with dim <= 2M on the complex128 Philox path), "plain" = complex128 with `start`; the small
+    sectors' chains in one fused launch; converged tridiagonal quadrature."""
     U, V, tp, mu, beta = (float(v) for v in theta)
     n = lat.Lx * lat.Ly
-    p = HubbardParams(lat.Lx, lat.Ly, lat.t, tp, U, V, lat.phi_x, lat.phi_y)
-    keys = [(nu, nd) for nu in range(n + 1) for nd in range(n + 1)]
-    secs = {k: Sector(p, *k) for k in keys}
-    limit = 2 * M if method == "batched" else FUSED_MAX_DIM
-    small = [k for k in keys if secs[k].dim() <= limit]
-    st = "philox" if method == "batched" else start
-    A, B, used = lanczos_sectors([secs[k] for k in small], R, M, seed, start=st)
-    out = {}
-    for i, k in enumerate(small):
-        out[k] = _quadrature(A[i * R:(i + 1) * R], B[i * R:(i + 1) * R], used[i * R:(i + 1) * R], beta,
-                             secs[k].dim())
-    for k in keys:
-        if k in out:
-            continue
-        s = secs[k]
-        if method == "batched":
-            a, b, u = s.batched_lanczos(R, M, seed)
-        else:
-            a, b, u = _plain_chains(s, R, M, seed, st)
-        out[k] = _quadrature(a, b, u, beta, s.dim())
-    for s in secs.values():
-        s.close()
-    lnz = np.array([out[k][0] for k in keys])
-    en = np.array([out[k][1] for k in keys])
-    N = np.array([nu + nd for nu, nd in keys], dtype=np.float64)
-    return lnz, en, N
+    nsec = (n + 1) ** 2
+    lnz = np.zeros(nsec)
+    en = np.zeros(nsec)
+    gc = C.c_double()
+    pc = _params(lat, U, V, tp)._c()
+    call("ftlm_gpu_gc_logz", C.byref(pc), mu, beta, int(R), int(M), C.c_uint(seed & 0xFFFFFFFF), METHODS[method],
+         START_MODES[start], _p(lnz), _p(en), C.byref(gc))
+    N = np.array([nu + nd for nu in range(n + 1) for nd in range(n + 1)], dtype=np.float64)
+    return lnz, en, N, gc.value
 
 
-def _plain_chains(s: Sector, R, M, seed, start):
-    A = np.zeros((R, M))
-    B = np.zeros((R, M))
-    used = np.zeros(R, np.int32)
-    for r in range(R):
-        a, b, u = s.lanczos(M, (seed + r * 100003) & 0xFFFFFFFF, start=start)
-        A[r, :a.size] = a
-        B[r, :b.size] = b
-        used[r] = u
-    return A, B, used
-
-
-def _sector_lnz(lat: Lattice, U, V, tp, beta, nu, nd, R, M, seed, method, start):
-    """One sector's ln Z_s, E_s (same chains and quadrature as sector_table)."""
-    s = Sector(HubbardParams(lat.Lx, lat.Ly, lat.t, tp, U, V, lat.phi_x, lat.phi_y), nu, nd)
-    if method == "batched" and s.dim() > 2 * M:
-        a, b, u = s.batched_lanczos(R, M, seed)
-    elif s.dim() <= (2 * M if method == "batched" else FUSED_MAX_DIM):
-        a, b, u = lanczos_sectors([s], R, M, seed, start="philox" if method == "batched" else start)
-    else:
-        a, b, u = _plain_chains(s, R, M, seed, "philox" if method == "batched" else start)
-    return _quadrature(a, b, u, beta, s.dim())
+def sector_table_grad(lat: Lattice, theta, R, M, seed, lnz, en, method="batched", start="reference"):
+    """d ln Z_GC / d(U, V, t', mu, beta) from the forward's sector table (ftlm_gpu_gc_logz_grad)."""
+    U, V, tp, mu, beta = (float(v) for v in theta)
+    g = np.zeros(5)
+    lnz = np.ascontiguousarray(lnz, np.float64)
+    en = np.ascontiguousarray(en, np.float64)
+    pc = _params(lat, U, V, tp)._c()
+    call("ftlm_gpu_gc_logz_grad", C.byref(pc), mu, beta, int(R), int(M), C.c_uint(seed & 0xFFFFFFFF),
+         METHODS[method], START_MODES[start], _p(lnz), _p(en), _p(g))
+    return g
 
 
 def _lse(x):
@@ -127,8 +87,7 @@ def _lse(x):
 
 
 def grand_canonical_logz_value(lat: Lattice, theta, R, M, seed, method="batched", start="reference") -> float:
-    lnz, _, N = sector_table(lat, theta, R, M, seed, method, start)
-    return _lse(lnz + float(theta[4]) * float(theta[3]) * N)
+    return sector_table(lat, theta, R, M, seed, method, start)[3]
 
 
 def gc_combine(lnz, en, N, mu: float, beta: float):
@@ -151,39 +110,19 @@ class GrandCanonicalLogZ(torch.autograd.Function):
     def forward(ctx, theta, lat: Lattice, R: int, M: int, seed: int, method: str = "batched",
                 start: str = "reference"):
         th = theta.detach().cpu().double().numpy()
-        lnz, en, N = sector_table(lat, th, R, M, seed, method, start)
-        lnZ = gc_combine(lnz, en, N, th[3], th[4])[0]
+        lnz, en, N, lnZ = sector_table(lat, th, R, M, seed, method, start)
         ctx.save_for_backward(theta)
         ctx.cfg = (lat, R, M, seed, method, start)
-        ctx.table = (lnz, en, N, lnZ)
+        ctx.table = (lnz, en)
         return theta.new_tensor(lnZ)
 
     @staticmethod
     def backward(ctx, grad_out):
         (theta,) = ctx.saved_tensors
         lat, R, M, seed, method, start = ctx.cfg
-        lnz, en, N, lnZ = ctx.table
-        U, V, tp, mu, beta = (float(v) for v in theta.detach().cpu().double().numpy())
-        _, w, dmu, dbeta = gc_combine(lnz, en, N, mu, beta)
-        d = np.zeros(3)
-        n = lat.Lx * lat.Ly
-        k = 0
-        for nu in range(n + 1):
-            for nd in range(n + 1):
-                ws = w[k]
-                k += 1
-                if not ws >= WEIGHT_CUTOFF:
-                    continue
-                p = HubbardParams(lat.Lx, lat.Ly, lat.t, tp, U, V, lat.phi_x, lat.phi_y)
-                s = Sector(p, nu, nd)
-                op = Sector(HubbardParams(lat.Lx, lat.Ly, 0.0, 1.0, 0.0, 0.0, lat.phi_x, lat.phi_y), nu, nd)
-                lz, g = s.ftlm_grad(beta, R, M, seed, op_tp=op, method=method, start=start)
-                if not abs(lz - lnz[k - 1]) <= 1e-9 * max(1.0, abs(lz)):
-                    raise RuntimeError(f"gradient replay of sector ({nu},{nd}) did not reproduce the forward "
-                                       f"ln Z ({lz} vs {lnz[k - 1]})")
-                d += ws * g
-        grad = theta.new_tensor([d[0], d[1], d[2], dmu, dbeta])
-        return grad_out * grad, None, None, None, None, None, None
+        lnz, en = ctx.table
+        g = sector_table_grad(lat, theta.detach().cpu().double().numpy(), R, M, seed, lnz, en, method, start)
+        return grad_out * theta.new_tensor(g), None, None, None, None, None, None
 
 
 def grand_canonical_logz(theta: torch.Tensor, lat: Lattice, R: int, M: int, seed: int, method: str = "batched",

@@ -21,6 +21,8 @@ LIB = os.path.join(HERE, "libftlm_gpu.so")
 DROPIN_LIB = os.path.join(HERE, "libftlm_dropin.so")
 DROPIN_SRC = os.path.join(HERE, "cpp", "dropin.cpp")
 DROPIN_INC = os.path.join(HERE, "cpp", "include")
+PYMOD_SRC = os.path.join(HERE, "python", "bindings.cpp")
+PYMOD_DIR = os.path.join(HERE, "python", "ftlm")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"] + ARCH
@@ -86,9 +88,46 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if force or _stale(DROPIN_LIB, [DROPIN_SRC, LIB, os.path.join(ROOT, "include", "ftlm_gpu.h")] + dhdrs):
         _run([cxx, *CXX_FLAGS, "-shared", "-I", DROPIN_INC, "-I", os.path.join(ROOT, "include"), DROPIN_SRC, "-o",
               DROPIN_LIB, "-L", HERE, "-lftlm_gpu", "-Wl,-rpath,$ORIGIN"])
+    build_pymodule(force)
     if verbose:
         print(LIB)
     return LIB
+
+
+def pymodule_path() -> str:
+    import sysconfig
+    return os.path.join(PYMOD_DIR, "_ftlm_core" + sysconfig.get_config_var("EXT_SUFFIX"))
+
+
+def build_pymodule(force: bool = False) -> str:
+    """The reference's pybind11 module _ftlm_core (python/ftlm/), compiled against torch's headers
+    (torch's own pybind11, its C++ ABI flag) and linked to libftlm_gpu.so + libftlm_dropin.so."""
+    import sysconfig
+
+    import torch
+    from torch.utils import cpp_extension as ce
+    out = pymodule_path()
+    deps = [PYMOD_SRC, LIB, DROPIN_LIB, os.path.join(ROOT, "include", "ftlm_gpu.h")]
+    if not force and not _stale(out, deps):
+        return out
+    incs = ce.include_paths() + [os.path.join(_cuda_home(), "include"), sysconfig.get_paths()["include"], DROPIN_INC,
+                                 os.path.join(ROOT, "include")]
+    abi = int(torch._C._GLIBCXX_USE_CXX11_ABI)
+    cmd = [_cxx(), "-O2", "-std=c++17", "-fPIC", "-shared", f"-D_GLIBCXX_USE_CXX11_ABI={abi}",
+           "-DTORCH_EXTENSION_NAME=_ftlm_core", "-DTORCH_API_INCLUDE_EXTENSION_H", "-fvisibility=hidden"]
+    for i in incs:
+        cmd += ["-isystem" if "torch" in i or "python" in i else "-I", i]
+    cmd += [PYMOD_SRC, "-o", out]
+    for lp in ce.library_paths():
+        cmd += ["-L", lp, f"-Wl,-rpath,{lp}"]
+    cmd += ["-lc10", "-lc10_cuda", "-ltorch", "-ltorch_cpu", "-ltorch_python", "-L", HERE, "-lftlm_dropin",
+            "-lftlm_gpu", "-Wl,-rpath,$ORIGIN/../.."]
+    _run(cmd)
+    return out
+
+
+def _cuda_home() -> str:
+    return os.path.dirname(os.path.dirname(_nvcc()))
 
 
 if __name__ == "__main__":

@@ -457,7 +457,7 @@ int ftlm_gpu_tridiag_eig(const double* alpha, const double* beta, const int* n, 
   if (nc < 0 || ld <= 0 || !alpha || !beta || !n || !lam || !w0) return fail(FTLM_ERR_INVALID, "bad arguments");
   if (ld > 160) return fail(FTLM_ERR_UNSUPPORTED, "tridiagonal size > 160 is not supported by the on-chip Jacobi");
   for (int c = 0; c < nc; ++c)
-    if (n[c] > ld) return fail(FTLM_ERR_INVALID, "chain length exceeds ld");
+    if (n[c] < 0 || n[c] > ld) return fail(FTLM_ERR_INVALID, "chain length outside [0, ld]");
   if (nc == 0) return FTLM_OK;
   const size_t mat = static_cast<size_t>(nc) * ld * sizeof(double);
   DevBuf da, db, dn, dl, dw;
@@ -481,6 +481,9 @@ int ftlm_gpu_tridiag_quadrature(const double* alpha, const double* beta, const i
   if (nc < 0 || ld <= 0 || n_bt < 0 || !alpha || !beta || !n || !bts || !logq || !energy)
     return fail(FTLM_ERR_INVALID, "bad arguments");
   if (ld > 160) return fail(FTLM_ERR_UNSUPPORTED, "tridiagonal size > 160 is not supported by the on-chip Jacobi");
+  for (int c = 0; c < nc; ++c)
+    if (n[c] < 0 || n[c] > ld) return fail(FTLM_ERR_INVALID, "chain length outside [0, ld]");
+  if (static_cast<long long>(nc) * n_bt > 0x7fffffffLL) return fail(FTLM_ERR_INVALID, "n_chains * n_bt exceeds 2^31 - 1");
   if (nc == 0 || n_bt == 0) return FTLM_OK;
   const size_t mat = static_cast<size_t>(nc) * ld * sizeof(double);
   const size_t outb = static_cast<size_t>(nc) * n_bt * sizeof(double);

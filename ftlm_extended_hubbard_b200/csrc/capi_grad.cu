@@ -245,6 +245,181 @@ int ftlm_gpu_grad_sector(ftlm_sector* s, ftlm_sector* op_tp, double bT, int R, i
   return FTLM_OK;
 }
 
+// ---- differentiable grand-canonical ln Z at one (T, mu) ----------------------------------------
+// Forward: every sector's chains as the FTLM entry points make them (the small sectors' chains in
+// one fused launch), the converged tridiagonal quadrature, the sector combine
+// (src/ftlm_thermo.cpp:246-256) and the grand-canonical log-sum-exp of
+// benchmarks/bench_ftlm_nmu_rect.cpp:186-219 at a single (T, mu).  Backward: d/dmu = bT <N>,
+// d/dbT = <mu N - E>, and d/d(U, V, t') = sum_s w_s d ln Z_s/dtheta from ftlm_gpu_grad_sector
+// (sectors with weight w_s < 1e-13 skipped).
+namespace {
+
+constexpr double kGcWeightCutoff = 1e-13;
+constexpr long long kGcFusedPlainMax = 1LL << 17;
+
+struct SectorDeleter {
+  void operator()(ftlm_sector* s) const { ftlm_gpu_sector_destroy(s); }
+};
+using SectorPtr = std::unique_ptr<ftlm_sector, SectorDeleter>;
+
+int gc_check(const ftlm_params* p, double bT, int R, int M, int method, int start_mode) {
+  if (!p) return fail(FTLM_ERR_INVALID, "null params");
+  const int n = p->Lx * p->Ly;
+  if (p->Lx <= 0 || p->Ly <= 0 || n > 32) return fail(FTLM_ERR_INVALID, "FockBasis: require 1 <= n_sites <= 32");
+  if (R <= 0 || M <= 0 || M > 160) return fail(FTLM_ERR_INVALID, "require R > 0 and 0 < M <= 160");
+  if (method < 0 || method > 1) return fail(FTLM_ERR_INVALID, "method must be 0 (plain) or 1 (batched)");
+  if (start_mode != FTLM_START_REFERENCE && start_mode != FTLM_START_PHILOX)
+    return fail(FTLM_ERR_INVALID, "unknown start_mode");
+  if (!(bT > 0.0) || !std::isfinite(bT)) return fail(FTLM_ERR_INVALID, "inverse temperature must be finite and > 0");
+  return FTLM_OK;
+}
+
+// ln Z_s, E_s at bT from R chains (alpha/beta [R][M], used [R]) of a sector of size dim.
+int gc_quadrature(const double* A, const double* B, const int* used, int R, int M, double bT, int64_t dim,
+                  double* lnz, double* en) {
+  std::vector<double> lq(static_cast<size_t>(R)), eq(static_cast<size_t>(R));
+  int rc = ftlm_gpu_tridiag_quadrature_exact(A, B, used, R, M, &bT, 1, lq.data(), eq.data());
+  if (rc) return rc;
+  return ftlm_gpu_ftlm_combine(lq.data(), eq.data(), used, R, 1, std::log(static_cast<double>(dim)), lnz, en);
+}
+
+double gc_lse(const std::vector<double>& x) {
+  double mx = -std::numeric_limits<double>::infinity();
+  for (double v : x) mx = std::max(mx, v);
+  if (!std::isfinite(mx)) return mx;
+  double s = 0.0;
+  for (double v : x) s += std::exp(v - mx);
+  return mx + std::log(s);
+}
+
+}  // namespace
+
+int ftlm_gpu_gc_logz(const ftlm_params* p, double mu, double bT, int R, int M, unsigned seed, int method,
+                     int start_mode, double* lnz_s, double* e_s, double* lnz_gc) {
+  int rc = gc_check(p, bT, R, M, method, start_mode);
+  if (rc) return rc;
+  if (!lnz_s || !e_s || !lnz_gc) return fail(FTLM_ERR_INVALID, "null output");
+  const int n = p->Lx * p->Ly;
+  const int nsec = (n + 1) * (n + 1);
+  const int st_mode = method == 1 ? FTLM_START_PHILOX : start_mode;
+  const long long limit = method == 1 ? 2LL * M : kGcFusedPlainMax;
+  std::vector<SectorPtr> small;
+  std::vector<int> small_idx;
+  std::vector<double> A, B;
+  std::vector<int> used;
+  for (int nu = 0; nu <= n; ++nu)
+    for (int nd = 0; nd <= n; ++nd) {
+      const int idx = nu * (n + 1) + nd;
+      ftlm_sector* raw = nullptr;
+      rc = ftlm_gpu_sector_create(p, nu, nd, &raw);
+      if (rc) return rc;
+      SectorPtr s(raw);
+      const int64_t dim = s->plan.dim;
+      if (dim <= limit) {  // chains of all small sectors in one launch below
+        small.push_back(std::move(s));
+        small_idx.push_back(idx);
+        continue;
+      }
+      if (method == 1) {
+        rc = need_device(s.get());
+        if (rc) return rc;
+        if (s->plan.max_up_deg > 120)
+          return fail(FTLM_ERR_UNSUPPORTED, "batched path: more than 120 up-hop sources per string");
+        rc = bt_run_chains(s.get(), R, M, seed, &A, &B, &used);
+        if (rc) return rc;
+      } else {
+        A.assign(static_cast<size_t>(R) * M, 0.0);
+        B.assign(static_cast<size_t>(R) * M, 0.0);
+        used.assign(static_cast<size_t>(R), 0);
+        for (int r = 0; r < R; ++r) {
+          int nb = 0, u = 0;
+          rc = ftlm_gpu_lanczos(s.get(), M, seed + static_cast<unsigned>(r) * 100003u, st_mode,
+                                A.data() + static_cast<size_t>(r) * M, B.data() + static_cast<size_t>(r) * M, &nb, &u);
+          if (rc) return rc;
+          used[static_cast<size_t>(r)] = u;
+        }
+      }
+      rc = gc_quadrature(A.data(), B.data(), used.data(), R, M, bT, dim, lnz_s + idx, e_s + idx);
+      if (rc) return rc;
+    }
+  if (!small.empty()) {
+    std::vector<ftlm_sector*> hs;
+    for (auto& s : small) hs.push_back(s.get());
+    const size_t ns = hs.size();
+    A.assign(ns * R * M, 0.0);
+    B.assign(ns * R * M, 0.0);
+    used.assign(ns * R, 0);
+    rc = ftlm_gpu_lanczos_sectors(hs.data(), static_cast<int>(ns), R, M, seed, st_mode, A.data(), B.data(), used.data());
+    if (rc) return rc;
+    for (size_t i = 0; i < ns; ++i) {
+      rc = gc_quadrature(A.data() + i * R * M, B.data() + i * R * M, used.data() + i * R, R, M, bT, hs[i]->plan.dim,
+                         lnz_s + small_idx[i], e_s + small_idx[i]);
+      if (rc) return rc;
+    }
+  }
+  std::vector<double> x(static_cast<size_t>(nsec));
+  for (int nu = 0; nu <= n; ++nu)
+    for (int nd = 0; nd <= n; ++nd) {
+      const int idx = nu * (n + 1) + nd;
+      x[static_cast<size_t>(idx)] = lnz_s[idx] + bT * mu * static_cast<double>(nu + nd);
+    }
+  *lnz_gc = gc_lse(x);
+  return FTLM_OK;
+}
+
+int ftlm_gpu_gc_logz_grad(const ftlm_params* p, double mu, double bT, int R, int M, unsigned seed, int method,
+                          int start_mode, const double* lnz_s, const double* e_s, double* grad) {
+  int rc = gc_check(p, bT, R, M, method, start_mode);
+  if (rc) return rc;
+  if (!lnz_s || !e_s || !grad) return fail(FTLM_ERR_INVALID, "null argument");
+  const int n = p->Lx * p->Ly;
+  const int nsec = (n + 1) * (n + 1);
+  std::vector<double> x(static_cast<size_t>(nsec)), N(static_cast<size_t>(nsec));
+  for (int nu = 0; nu <= n; ++nu)
+    for (int nd = 0; nd <= n; ++nd) {
+      const int idx = nu * (n + 1) + nd;
+      N[static_cast<size_t>(idx)] = static_cast<double>(nu + nd);
+      x[static_cast<size_t>(idx)] = lnz_s[idx] + bT * mu * N[static_cast<size_t>(idx)];
+    }
+  const double lnZ = gc_lse(x);
+  if (!std::isfinite(lnZ)) return fail(FTLM_ERR_NUMERIC, "grand-canonical ln Z is not finite");
+  double d[3] = {0.0, 0.0, 0.0}, dmu = 0.0, dbeta = 0.0;
+  ftlm_params pop = *p;  // dH/dt': the t' hopping operator alone
+  pop.t = 0.0;
+  pop.tp = 1.0;
+  pop.U = 0.0;
+  pop.V = 0.0;
+  for (int nu = 0; nu <= n; ++nu)
+    for (int nd = 0; nd <= n; ++nd) {
+      const size_t idx = static_cast<size_t>(nu * (n + 1) + nd);
+      const double w = std::exp(x[idx] - lnZ);
+      if (!(w > 0.0)) continue;
+      dmu += bT * w * N[idx];
+      dbeta += w * (mu * N[idx] - e_s[idx]);
+      if (!(w >= kGcWeightCutoff)) continue;
+      ftlm_sector *rs = nullptr, *ro = nullptr;
+      rc = ftlm_gpu_sector_create(p, nu, nd, &rs);
+      if (rc) return rc;
+      SectorPtr s(rs);
+      rc = ftlm_gpu_sector_create(&pop, nu, nd, &ro);
+      if (rc) return rc;
+      SectorPtr op(ro);
+      double lz = 0.0, g[3] = {0.0, 0.0, 0.0};
+      rc = ftlm_gpu_grad_sector(s.get(), op.get(), bT, R, M, seed, method, start_mode, &lz, g);
+      if (rc) return rc;
+      if (!(std::fabs(lz - lnz_s[idx]) <= 1e-9 * std::max(1.0, std::fabs(lz))))
+        return fail(FTLM_ERR_NUMERIC, "gradient replay of sector (" + std::to_string(nu) + "," + std::to_string(nd) +
+                                          ") did not reproduce the forward ln Z");
+      for (int q = 0; q < 3; ++q) d[q] += w * g[q];
+    }
+  grad[0] = d[0];
+  grad[1] = d[1];
+  grad[2] = d[2];
+  grad[3] = dmu;
+  grad[4] = dbeta;
+  return FTLM_OK;
+}
+
 // Per-chain log quadrature and energy ratio with a converged eigen-decomposition (host QL), the
 // quadrature the gradient differentiates; same layout as ftlm_gpu_tridiag_quadrature.
 int ftlm_gpu_tridiag_quadrature_exact(const double* alpha, const double* beta, const int* n, int nc, int ld,

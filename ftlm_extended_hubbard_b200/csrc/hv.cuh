@@ -39,11 +39,12 @@ cudaError_t lz_normalise_start(double2* q, int64_t n, const double* scratch, cud
 
 // ---- quadrature (quad.cu) ----
 // Batched classical Jacobi, one CTA per chain: alpha/beta [nc][ld], n[nc]; outputs lam/w0 [nc][ld].
+// A chain with n outside [0, ld] is skipped and sets *bad (when bad is given).
 cudaError_t quad_jacobi(const double* alpha, const double* beta, const int* n, int nc, int ld, int max_rot,
-                        double tol, double* lam, double* w0, cudaStream_t st);
-// logq/energy [nc][nbt] from lam/w0.
+                        double tol, double* lam, double* w0, cudaStream_t st, int* bad = nullptr);
+// logq/energy [nc][nbt] from lam/w0; a chain with n outside [0, ld] gets NaN and sets *bad.
 cudaError_t quad_eval(const double* lam, const double* w0, const int* n, int nc, int ld, const double* bts, int nbt,
-                      double* logq, double* energy, cudaStream_t st);
+                      double* logq, double* energy, cudaStream_t st, int* bad = nullptr);
 // Sector ln Z from R chain values: lnz[b] = ln(dim) + log mean_r exp(logq[r][b]); energy weighted.
 cudaError_t quad_sector(const double* logq, const double* eq, const int* n, int R, int nbt, double log_dim,
                         double* lnz, double* energy, cudaStream_t st);

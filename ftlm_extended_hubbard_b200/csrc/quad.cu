@@ -28,15 +28,21 @@ __global__ void __launch_bounds__(kJacThreads) jacobi_kernel(const double* __res
                                                              const double* __restrict__ beta,
                                                              const int* __restrict__ nv, int ld, int max_rot_in,
                                                              double tol, double* __restrict__ lam,
-                                                             double* __restrict__ w0) {
+                                                             double* __restrict__ w0, int* __restrict__ bad) {
   extern __shared__ double sm[];
   __shared__ double red_v[kJacThreads / 32];
   __shared__ int red_i[kJacThreads / 32];
   __shared__ double s_c, s_s, s_app, s_aqq, s_apq;
   __shared__ int s_p, s_q, s_stop;
   const int ch = blockIdx.x;
-  const int n = nv[ch];
+  int n = nv[ch];
   const int tid = threadIdx.x;
+  // A chain length outside [0, ld] would overrun the ld x ld shared matrix and the chain's rows of
+  // alpha/beta/lam/w0: such a chain is skipped and reported through *bad (when given).
+  if (n < 0 || n > ld) {
+    if (tid == 0 && bad) atomicOr(bad, 1);
+    n = 0;
+  }
   const double* a = alpha + static_cast<int64_t>(ch) * ld;
   const double* b = beta + static_cast<int64_t>(ch) * ld;
   double* lo = lam + static_cast<int64_t>(ch) * ld;
@@ -154,16 +160,20 @@ __global__ void __launch_bounds__(kJacThreads) jacobi_kernel(const double* __res
 // src/ftlm_thermo.cpp:124-146 (log-sum-exp over Ritz pairs with w > 0) and the energy ratio.
 __global__ void eval_kernel(const double* __restrict__ lam, const double* __restrict__ w0, const int* __restrict__ nv,
                             int nc, int ld, const double* __restrict__ bts, int nbt, double* __restrict__ logq,
-                            double* __restrict__ energy) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nc * nbt) return;
-  const int ch = i / nbt, bi = i - ch * nbt;
+                            double* __restrict__ energy, int* __restrict__ bad) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= static_cast<int64_t>(nc) * nbt) return;
+  const int ch = static_cast<int>(i / nbt), bi = static_cast<int>(i - static_cast<int64_t>(ch) * nbt);
   const int n = nv[ch];
   const double bT = bts[bi];
   const double* l = lam + static_cast<int64_t>(ch) * ld;
   const double* w = w0 + static_cast<int64_t>(ch) * ld;
   double out = -CUDART_INF, e = 0.0;
-  if (n == 1) {
+  if (n < 0 || n > ld) {  // invalid chain length (see jacobi_kernel): NaN outputs, reported
+    if (bad) atomicOr(bad, 1);
+    out = CUDART_NAN;
+    e = CUDART_NAN;
+  } else if (n == 1) {
     out = -bT * l[0];
     e = l[0];
   } else if (n > 1) {
@@ -296,20 +306,22 @@ __global__ void ritz_kernel(const double* __restrict__ a, const double* __restri
 }  // namespace
 
 cudaError_t quad_jacobi(const double* alpha, const double* beta, const int* n, int nc, int ld, int max_rot,
-                        double tol, double* lam, double* w0, cudaStream_t st) {
+                        double tol, double* lam, double* w0, cudaStream_t st, int* bad) {
   if (nc <= 0) return cudaSuccess;
   const size_t sm = (static_cast<size_t>(ld) * ld + ld) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
   if (e != cudaSuccess) return e;
-  jacobi_kernel<<<nc, kJacThreads, sm, st>>>(alpha, beta, n, ld, max_rot, tol, lam, w0);
+  jacobi_kernel<<<nc, kJacThreads, sm, st>>>(alpha, beta, n, ld, max_rot, tol, lam, w0, bad);
   return cudaGetLastError();
 }
 
 cudaError_t quad_eval(const double* lam, const double* w0, const int* n, int nc, int ld, const double* bts, int nbt,
-                      double* logq, double* energy, cudaStream_t st) {
-  const int tot = nc * nbt;
+                      double* logq, double* energy, cudaStream_t st, int* bad) {
+  const int64_t tot = static_cast<int64_t>(nc) * nbt;
   if (tot <= 0) return cudaSuccess;
-  eval_kernel<<<(tot + 127) / 128, 128, 0, st>>>(lam, w0, n, nc, ld, bts, nbt, logq, energy);
+  if ((tot + 127) / 128 > 0x7fffffffLL) return cudaErrorInvalidValue;
+  eval_kernel<<<static_cast<unsigned>((tot + 127) / 128), 128, 0, st>>>(lam, w0, n, nc, ld, bts, nbt, logq, energy,
+                                                                       bad);
   return cudaGetLastError();
 }
 

@@ -142,10 +142,13 @@ int ftlm_gpu_tridiag_quadrature(const double* alpha, const double* beta, const i
  * another allocator (e.g. a framework pool that has reserved most of HBM) or latency-critical loops
  * where allocation would implicitly synchronise the device.  Intermediate Ritz pairs live in a
  * library-owned 1 MiB __device__ array on every GPU that loads the library: n_chains*ld <= 65536,
- * larger requests fail with FTLM_ERR_UNSUPPORTED.  Calls that overlap on the GPU race on that array
- * (serialise them on one stream).  The first call on each device looks the array up with
- * cudaGetSymbolAddress; make it before any stream capture on that device.  Work is enqueued on
- * `stream`; the call does not synchronise. */
+ * larger requests fail with FTLM_ERR_UNSUPPORTED.  Requires 0 <= n_dev[c] <= ld: a chain outside
+ * that range is skipped (its outputs become NaN) and the call returns FTLM_ERR_INVALID.  Calls that
+ * overlap on the GPU race on that array (serialise them on one stream).  The first call on each
+ * device (and the first after that device's context is recreated, e.g. by cudaDeviceReset) looks
+ * the array up with cudaGetSymbolAddress; make it before any stream capture on that device.  Work
+ * is enqueued on `stream`, and the call waits for that stream only, to read back the chain-length
+ * check (no device-wide synchronisation). */
 int ftlm_gpu_tridiag_quadrature_noalloc(const double* alpha_dev, const double* beta_dev, const int* n_dev, int n_chains,
                                         int ld, const double* bts_dev, int n_bt, double* logq_dev, double* energy_dev,
                                         void* stream);
@@ -266,6 +269,20 @@ int ftlm_gpu_orbit_sector_batched_ftlm(ftlm_sector* s, const double* bts, int n_
  * sector, twice with op_tp; released by ftlm_gpu_batched_release. */
 int ftlm_gpu_grad_sector(ftlm_sector* s, ftlm_sector* op_tp, double bT, int R, int M, unsigned seed, int method,
                          int start_mode, double* lnz, double* dlnz);
+/* Differentiable grand-canonical ln Z at one point (no reference counterpart; the combination is the
+ * grand-canonical reduction of benchmarks/bench_ftlm_nmu_rect.cpp:186-219 at a single (T, mu)).
+ * p gives the lattice and (t, t', U, V, phi_x, phi_y); every (N_up, N_dn) sector's FTLM ln Z_s and
+ * energy E_s at inverse temperature bT (method 0: complex128 chains with start_mode; method 1: the
+ * batched complex64 chains; converged tridiagonal quadrature; the small sectors' chains in one fused
+ * launch) go to lnz_s/e_s [(n+1)^2] in sector order nu*(n+1)+nd, and
+ * lnz_gc = log sum_s exp(ln Z_s + bT mu (N_up + N_dn)). */
+int ftlm_gpu_gc_logz(const ftlm_params* p, double mu, double bT, int R, int M, unsigned seed, int method,
+                     int start_mode, double* lnz_s, double* e_s, double* lnz_gc);
+/* Its gradient grad[5] = d lnz_gc / d(U, V, t', mu, bT) from the forward's sector table, the chains
+ * replayed from their seeds (ftlm_gpu_grad_sector; sectors of weight < 1e-13 skipped).  Fails with
+ * FTLM_ERR_NUMERIC if a replay does not reproduce the forward's ln Z_s. */
+int ftlm_gpu_gc_logz_grad(const ftlm_params* p, double mu, double bT, int R, int M, unsigned seed, int method,
+                          int start_mode, const double* lnz_s, const double* e_s, double* grad);
 /* Host-only dense helpers behind the gradient (no reference counterpart): eigen-decomposition of
  * a symmetric tridiagonal (implicit QL; lam ascending, Z row-major with eigenvectors in columns),
  * and the Duhamel weight matrix K (n x n) with g = e_1^T e^{-bT (T - lam_min)} e_1. */

@@ -17,7 +17,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "libftlm_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libftlm_ref.so")
-REFERENCE_SRC = "/root/reference"
+# Where the reference checkout lives: $FTLM_REFERENCE_SRC, else a sibling checkout named "reference"
+# next to this repository.  Only building the checker reads it; the built libraries travel.
+REFERENCE_SRC = os.environ.get("FTLM_REFERENCE_SRC") or os.path.normpath(
+    os.path.join(HERE, os.pardir, os.pardir, "reference"))
 
 _d, _i, _vp, _ll = C.c_double, C.c_int, C.c_void_p, C.c_longlong
 

@@ -13,6 +13,15 @@ published_korbit.npz  the reference's published k-orbit run on 3x2 (benchmarks/d
 orbit_small.npz    translation-orbit momentum blocks from the reference library (OrbitKBlockBasis::build,
                    apply_orbit_k_block, ftlm_log_partition_complex): representatives, |A|, orbit sizes,
                    H_K x on seeded vectors and block ln Z.
+ritz_4x4_8_8.npz   the 4x4 (8,8) Lanczos chain of the single-sector workload (dim 165,636,900,
+                   t=1 t'=-0.25 U=8 V=1 phi_x=0.1, reference start vector seed 7, M=150): alpha, beta
+                   and the lowest 5 Ritz values, computed by the oracle's threaded row gather with the
+                   reference recurrence (about 1.5-2 h on 8 host threads; made only on request:
+                   `python tests/golden/make_golden.py ritz_4x4_8_8`).
+ed_4x2.npz         full exact diagonalisation of the 4x2 lattice (t=1 t'=-0.25 U=8 V=1, phi=0, all 65,536
+                   levels) by the reference's own NumPy ED mirror (benchmarks/hubbard_rect_ed.py,
+                   imported from the reference checkout): exact per-sector ln Z and ln Z_GC / <n> on
+                   the T x mu grid of sweep_4x2 (a few minutes; `python tests/golden/make_golden.py ed_4x2`).
 sweep_4x2.npz    the plain FTLM sweep of 4x2, t=1 t'=-0.25 U=8 V=1, phi=0, R=20, M=60, seed 7,
                    T = 0.1..2.0 (20) x mu = -4..8 (49), computed by the oracle in the reference's
                    scatter order (bit-identical to the reference library; this script checks the
@@ -209,7 +218,83 @@ def sweep_4x2():
                                 c["M"], c["seed"]], dtype=np.float64)}
 
 
+RITZ_4X4 = (4, 4, 1.0, -0.25, 8.0, 1.0, 0.1, 0.0, 8, 8)
+
+
+def ritz_4x4_8_8(nthreads=None):
+    """The single-sector workload's chain (src/lanczos.cpp:125-208 restated, threaded gather H·v)."""
+    import time
+    nthreads = nthreads or os.cpu_count() or 8
+    s = O.OracleSector(*RITZ_4X4)
+    t0 = time.time()
+    a, b, used = s.lanczos(150, 7, mode=1, nthreads=nthreads)
+    secs = time.time() - t0
+    n = len(a)
+    T = np.diag(a) + np.diag(b[:n - 1], 1) + np.diag(b[:n - 1], -1)
+    ritz = np.linalg.eigvalsh(T)[:5]
+    return {"params": np.array(RITZ_4X4, np.float64), "M": np.array([150]), "seed": np.array([7]),
+            "alpha": a, "beta": b, "used": np.array([used]), "ritz5": ritz, "seconds": np.array([secs]),
+            "threads": np.array([nthreads])}
+
+
+ED_4X2 = dict(t=1.0, tp=-0.25, U=8.0, V=1.0)
+
+
+def ed_4x2():
+    """Exact spectrum of every (N_up, N_dn) sector of 4x2 from the reference's NumPy ED mirror
+    (benchmarks/hubbard_rect_ed.py:45-213); the grand-canonical reduction follows its
+    grand_canonical_n (log-sum-exp over all levels)."""
+    sys.path.insert(0, os.path.join(O.REFERENCE_SRC, "benchmarks"))
+    import hubbard_rect_ed as ED  # the reference's own ED script
+    lx, ly = 4, 2
+    n = lx * ly
+    hops, pairs = ED.build_hubbard_geometry_py(lx, ly, ED_4X2["t"], ED_4X2["tp"], 0.0, 0.0)
+    betas = 1.0 / T_GRID
+    lnz_s = np.full(((n + 1) ** 2, betas.size), -np.inf)
+    N = np.zeros((n + 1) ** 2, np.int32)
+    levels = []
+    for nu in range(n + 1):
+        for nd in range(n + 1):
+            idx = nu * (n + 1) + nd
+            N[idx] = nu + nd
+            basis = ED.enumerate_sector(n, nu, nd)
+            h = ED.build_h_sector(basis, hops, pairs, ED_4X2["U"], ED_4X2["V"])
+            w = np.linalg.eigvalsh((h + np.conjugate(h.T)) * 0.5)
+            levels.append((w, nu + nd))
+            for bi, b in enumerate(betas):
+                a = -b * w
+                m = a.max()
+                lnz_s[idx, bi] = m + np.log(np.exp(a - m).sum())
+    lnz_gc = np.zeros((betas.size, MU_GRID.size))
+    n_gc = np.zeros_like(lnz_gc)
+    E = np.concatenate([w for w, _ in levels])
+    Nl = np.concatenate([np.full(w.size, k, np.float64) for w, k in levels])
+    for bi, b in enumerate(betas):
+        for mi, mu in enumerate(MU_GRID):
+            a = -b * (E - mu * Nl)
+            m = a.max()
+            wts = np.exp(a - m)
+            lnz_gc[bi, mi] = m + np.log(wts.sum())
+            n_gc[bi, mi] = (Nl * wts).sum() / wts.sum() / n
+            # cross-check against the reference script's own reduction on a few points
+            if bi % 9 == 0 and mi % 16 == 0:
+                ref_n = ED.grand_canonical_n(float(b), float(mu), list(zip(E.tolist(), Nl.astype(int).tolist())), n)
+                assert abs(ref_n - n_gc[bi, mi]) < 1e-12, (b, mu, ref_n, n_gc[bi, mi])
+    return {"lnz_sector": lnz_s, "N": N, "T": T_GRID, "mu": MU_GRID, "lnz_gc": lnz_gc, "n_gc": n_gc,
+            "params": np.array([lx, ly, ED_4X2["t"], ED_4X2["tp"], ED_4X2["U"], ED_4X2["V"], 0.0, 0.0])}
+
+
+ON_REQUEST = {"ritz_4x4_8_8": ritz_4x4_8_8, "ed_4x2": ed_4x2}
+
+
 def main():
+    wanted = [a for a in sys.argv[1:] if a in ON_REQUEST]
+    if wanted:
+        O.build(ref=False)
+        for name in wanted:
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), **ON_REQUEST[name]())
+            print("wrote", name + ".npz")
+        return
     O.build(ref=True)
     np.savez_compressed(os.path.join(HERE, "published_tsv.npz"), **published())
     np.savez_compressed(os.path.join(HERE, "ref_small.npz"), **ref_small())

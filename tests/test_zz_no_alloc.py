@@ -9,7 +9,10 @@ the intermediate Ritz pairs in its own fixed 1 MiB device array.
 Checked here, through the C ABI: the output equals the allocating entry point
 (ftlm_gpu_tridiag_quadrature) within the tests' thermodynamic tolerance on two calls in a row with
 different inputs (the shared scratch carries nothing over), the second call changes no device
-allocation, and requests larger than the scratch are rejected before any GPU work.
+allocation, and requests larger than the scratch are rejected before any GPU work.  Edge cases:
+a batch that fills the scratch exactly (512 chains x ld 128), the largest ld (160), chains of
+length 0 (-inf, as the allocating path), work queued on a side stream behind other work, and a
+device-resident chain length above ld (skipped in-bounds, NaN outputs, FTLM_ERR_INVALID).
 This file is named so that pytest collects it last.
 """
 import ctypes as C
@@ -25,10 +28,11 @@ pytestmark = pytest.mark.gpu
 RTOL_THERMO = 1e-10
 
 
-def _batch(seed, n_chains, ld):
+def _batch(seed, n_chains, ld, n_zero=0):
     rng = np.random.default_rng(seed)
     n = rng.integers(1, ld + 1, n_chains).astype(np.int32)
     n[0] = ld
+    n[1:1 + n_zero] = 0
     A = np.zeros((n_chains, ld))
     B = np.zeros((n_chains, ld))
     for c in range(n_chains):
@@ -78,3 +82,76 @@ def test_noalloc_rejects_oversized_batch(gpu):
                   C.c_void_p(x.data_ptr()), None)
     assert e.value.code == _lib.FTLM_ERR_UNSUPPORTED
     assert "65536" in str(e.value)
+
+
+def _noalloc(torch, A, B, n, bts, stream, n_override=None):
+    n_chains, ld = A.shape
+    a_d = torch.tensor(A, device="cuda")
+    b_d = torch.tensor(B, device="cuda")
+    n_d = torch.tensor(n if n_override is None else n_override, device="cuda")
+    bts_d = torch.tensor(bts, dtype=torch.float64, device="cuda")
+    q_d = torch.full((n_chains, bts.size), 7.0, dtype=torch.float64, device="cuda")
+    e_d = torch.full_like(q_d, 7.0)
+    err = None
+    try:
+        _lib.call("ftlm_gpu_tridiag_quadrature_noalloc", C.c_void_p(a_d.data_ptr()), C.c_void_p(b_d.data_ptr()),
+                  C.c_void_p(n_d.data_ptr()), n_chains, ld, C.c_void_p(bts_d.data_ptr()), bts.size,
+                  C.c_void_p(q_d.data_ptr()), C.c_void_p(e_d.data_ptr()), C.c_void_p(stream.cuda_stream))
+    except F.FtlmError as ex:
+        err = ex
+    torch.cuda.synchronize()
+    return q_d.cpu().numpy(), e_d.cpu().numpy(), err
+
+
+def _close(x, ref):
+    fin = np.isfinite(ref)
+    assert np.array_equal(fin, np.isfinite(x))
+    assert np.array_equal(x[~fin], ref[~fin])
+    return np.all(np.abs(x[fin] - ref[fin]) <= RTOL_THERMO * np.maximum(1.0, np.abs(ref[fin])))
+
+
+@pytest.mark.parametrize("n_chains,ld,n_zero", [(512, 128, 3), (5, 160, 1)])
+def test_noalloc_edges_full_scratch_max_ld_empty_chains(gpu, n_chains, ld, n_zero):
+    torch = gpu
+    bts = np.array([0.1, 1.0, 10.0])
+    A, B, n = _batch(40 + ld, n_chains, ld, n_zero)
+    ref_q, ref_e = F.tridiag_quadrature(A, B, n, bts)
+    assert np.all(np.isneginf(ref_q[1:1 + n_zero]))
+    q, e, err = _noalloc(torch, A, B, n, bts, torch.cuda.current_stream())
+    assert err is None
+    assert _close(q, ref_q) and _close(e, ref_e)
+
+
+def test_noalloc_on_side_stream_behind_other_work(gpu):
+    torch = gpu
+    bts = np.array([0.3, 3.0])
+    A, B, n = _batch(77, 64, 90)
+    ref_q, ref_e = F.tridiag_quadrature(A, B, n, bts)
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        big = torch.randn(1 << 24, device="cuda")
+        for _ in range(4):  # queued work the quadrature has to wait behind
+            big = big * 1.0001 + 0.5
+        q, e, err = _noalloc(torch, A, B, n, bts, side)
+    assert err is None
+    assert _close(q, ref_q) and _close(e, ref_e)
+
+
+def test_noalloc_chain_longer_than_ld_is_reported(gpu):
+    """A device-resident chain length of ld + 1 cannot be checked on the host: the kernels skip
+    that chain without touching memory past its rows, set its outputs to NaN and the call returns
+    FTLM_ERR_INVALID; the other chains are still correct, and the next call works normally."""
+    torch = gpu
+    bts = np.array([0.5, 2.0])
+    ld = 40
+    A, B, n = _batch(5, 6, ld)
+    bad = n.copy()
+    bad[2] = ld + 1
+    ref_q, ref_e = F.tridiag_quadrature(A, B, n, bts)
+    q, e, err = _noalloc(torch, A, B, n, bts, torch.cuda.current_stream(), n_override=bad)
+    assert err is not None and err.code == _lib.FTLM_ERR_INVALID
+    assert np.all(np.isnan(q[2])) and np.all(np.isnan(e[2]))
+    keep = np.arange(6) != 2
+    assert _close(q[keep], ref_q[keep]) and _close(e[keep], ref_e[keep])
+    q, e, err = _noalloc(torch, A, B, n, bts, torch.cuda.current_stream())
+    assert err is None and _close(q, ref_q) and _close(e, ref_e)
