@@ -57,6 +57,8 @@ def parse():
                          "grand-canonical sweep, batched complex64 and plain complex128 (same Philox starts), "
                          "R=32, M=100, T=0.1..2 x mu=-4..8 (tens of minutes)")
     ap.add_argument("--k", type=int, nargs=2, default=(1, 2), metavar=("KX", "KY"), help="orbit workload momentum")
+    ap.add_argument("--check", type=int, default=1,
+                    help="sweep workload: chains per sector rerun in complex128 for the per-result error estimate")
     return ap.parse_args()
 
 
@@ -560,27 +562,36 @@ def run_published(args):
 
 def run_sweep(args):
     """The full 4x4 sweep (289 sectors, R=32, M=100) with both paths, end to end, and the batched
-    path's errors against complex128 with the same Philox start vectors."""
+    path's errors against complex128 with the same Philox start vectors (both with the converged
+    quadrature): measured against the plain sweep, and the batched path's own per-result estimate
+    (chain 0 of every sector rerun in complex128, --check 1)."""
     import numpy as np
     import ftlm_extended_hubbard_b200 as F
     p = F.HubbardParams(**PARAMS)
     T = np.round(np.arange(1, 21) * 0.1, 10)
     mu = np.round(np.arange(49) * 0.25 - 4.0, 10)
     t0 = time.perf_counter()
-    rb = F.grand_canonical_sweep(p, 32, 100, 7, T, mu, method="batched")
+    rb = F.grand_canonical_sweep(p, 32, 100, 7, T, mu, method="batched", check=args.check)
     tb = time.perf_counter() - t0
     F.batched_release()
     t0 = time.perf_counter()
-    rp = F.grand_canonical_sweep(p, 32, 100, 7, T, mu, start="philox")
+    with F.quadrature("converged"):
+        rp = F.grand_canonical_sweep(p, 32, 100, 7, T, mu, start="philox")
     tp = time.perf_counter() - t0
     ok = np.isfinite(rp.lnz_sector)
     rel_s = np.abs(rb.lnz_sector[ok] - rp.lnz_sector[ok]) / np.maximum(1.0, np.abs(rp.lnz_sector[ok]))
     rel_g = np.abs(rb.lnz_gc - rp.lnz_gc) / np.maximum(1.0, np.abs(rp.lnz_gc))
-    print(json.dumps({"workload": "full 4x4 grand-canonical sweep, 289 sectors, R=32, M=100, T 0.1..2 (20) x mu "
-                                  "-4..8 (49), t=1 t'=-0.25 U=8 V=1 phi_x=0.1",
-                      "batched_s": tb, "plain_s": tp, "ratio": tp / tb,
-                      "max_rel_err_sector_lnz": float(rel_s.max()), "max_rel_err_gc_lnz": float(rel_g.max()),
-                      "max_abs_err_n": float(np.abs(rb.n_avg - rp.n_avg).max())}))
+    out = {"workload": "full 4x4 grand-canonical sweep, 289 sectors, R=32, M=100, T 0.1..2 (20) x mu "
+                       "-4..8 (49), t=1 t'=-0.25 U=8 V=1 phi_x=0.1",
+           "batched_s": tb, "plain_s": tp, "ratio": tp / tb, "check_chains": args.check,
+           "max_rel_err_sector_lnz": float(rel_s.max()), "max_rel_err_gc_lnz": float(rel_g.max()),
+           "max_abs_err_n": float(np.abs(rb.n_avg - rp.n_avg).max())}
+    if rb.lnz_gc_err is not None:
+        out["estimated_max_rel_err_sector_lnz"] = float(
+            (rb.lnz_sector_err[ok] / np.maximum(1.0, np.abs(rp.lnz_sector[ok]))).max())
+        out["estimated_max_rel_err_gc_lnz"] = float((rb.lnz_gc_err / np.maximum(1.0, np.abs(rb.lnz_gc))).max())
+        out["estimated_max_abs_err_n"] = float(rb.n_err.max())
+    print(json.dumps(out))
     return 0
 
 

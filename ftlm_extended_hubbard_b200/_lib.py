@@ -13,6 +13,8 @@ LIB_PATH = os.path.join(HERE, "libftlm_gpu.so")
 
 FTLM_OK = 0
 FTLM_ERR_INVALID = 1
+FTLM_QUAD_REFERENCE = 0
+FTLM_QUAD_CONVERGED = 1
 FTLM_ERR_CUDA = 2
 FTLM_ERR_NOMEM = 3
 FTLM_ERR_TIMEOUT = 4
@@ -70,6 +72,7 @@ SIGNATURES = {
     "ftlm_gpu_sector_stats": [_vp, _pd, _pd, C.POINTER(_ll), C.POINTER(_ll)],
     "ftlm_gpu_sector_diag": [_vp, _ll, _pd],
     "ftlm_gpu_sector_down_table": [_vp, C.POINTER(_ll), C.POINTER(_ll), _vp, _vp, _pi],
+    "ftlm_gpu_sector_down_table_compact": [_vp, _pi, C.POINTER(_ll), C.POINTER(_ll), _vp, _vp, _vp, _vp, _pi, _pi],
     "ftlm_gpu_apply": [_vp, _vp, _vp, _vp],
     "ftlm_gpu_apply_host": [_vp, _vp, _vp],
     "ftlm_gpu_apply_profiled": [_vp, _vp, _vp, _vp, C.POINTER(C.c_float), _pi],
@@ -87,7 +90,11 @@ SIGNATURES = {
     "ftlm_gpu_batched_ftlm_sector": [_vp, _vp, _i, _i, _i, C.c_uint, _vp, _vp],
     "ftlm_gpu_batched_sweep": [C.POINTER(FtlmParams), _i, _i, C.c_uint, _vp, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp],
     "ftlm_gpu_batched_release": [],
+    "ftlm_gpu_batched_ftlm_sector_checked": [_vp, _vp, _i, _i, _i, C.c_uint, _i, _vp, _vp, _vp],
+    "ftlm_gpu_batched_sweep_checked": [C.POINTER(FtlmParams), _i, _i, C.c_uint, _vp, _i, _vp, _i, _i, _vp, _vp, _vp,
+                                       _vp, _vp, _vp, _vp, _vp],
     "ftlm_gpu_set_fused_max_dim": [_ll],
+    "ftlm_gpu_set_quadrature": [_i],
     "ftlm_gpu_autotune_apply": [_vp, _i, _vp, _vp, _vp],
     "ftlm_gpu_set_cols_variant": [_vp, _i],
     "ftlm_gpu_lanczos_sectors": [_vp, _i, _i, _i, C.c_uint, _i, _vp, _vp, _vp],

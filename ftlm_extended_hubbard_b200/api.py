@@ -280,10 +280,18 @@ class Sector(_Handle):
              b.ctypes.data_as(C.c_void_p), u.ctypes.data_as(C.c_void_p))
         return a, b, u
 
-    def batched_ftlm(self, betas, n_random: int, lanczos_steps: int, seed: int):
+    def batched_ftlm(self, betas, n_random: int, lanczos_steps: int, seed: int, check: int = 0):
+        """Batched complex64 sector FTLM: (ln Z, E); with check > 0 also the estimated rounding error
+        of ln Z against complex128 (chains r < check rerun in complex128): (ln Z, E, err)."""
         bt = np.ascontiguousarray(np.atleast_1d(np.asarray(betas, dtype=np.float64)))
         lnz = np.zeros(bt.size)
         en = np.zeros(bt.size)
+        if check > 0:
+            err = np.zeros(bt.size)
+            call("ftlm_gpu_batched_ftlm_sector_checked", self._h, bt.ctypes.data_as(C.c_void_p), bt.size, n_random,
+                 lanczos_steps, C.c_uint(seed & 0xFFFFFFFF), int(check), lnz.ctypes.data_as(C.c_void_p),
+                 en.ctypes.data_as(C.c_void_p), err.ctypes.data_as(C.c_void_p))
+            return lnz, en, err
         call("ftlm_gpu_batched_ftlm_sector", self._h, bt.ctypes.data_as(C.c_void_p), bt.size, n_random,
              lanczos_steps, C.c_uint(seed & 0xFFFFFFFF), lnz.ctypes.data_as(C.c_void_p), en.ctypes.data_as(C.c_void_p))
         return lnz, en
@@ -475,6 +483,32 @@ def batched_release():
     call("ftlm_gpu_batched_release")
 
 
+QUADRATURES = {"reference": 0, "converged": 1}
+
+
+def set_quadrature(mode: str) -> None:
+    """Quadrature of the complex128 sector path: "reference" (default; the reference's rotation-capped
+    Jacobi, src/ftlm_thermo.cpp:83-146) or "converged" (the converged GPU Jacobi, which the batched
+    complex64 path always uses).  Process-wide."""
+    call("ftlm_gpu_set_quadrature", QUADRATURES[mode])
+
+
+class quadrature:
+    """Context manager: `with quadrature("converged"): ...` sets the complex128 path's quadrature and
+    restores the reference quadrature on exit."""
+
+    def __init__(self, mode: str):
+        self.mode = mode
+
+    def __enter__(self):
+        set_quadrature(self.mode)
+        return self
+
+    def __exit__(self, *exc):
+        set_quadrature("reference")
+        return False
+
+
 def tridiag_eig(alpha: np.ndarray, beta: np.ndarray, n: np.ndarray, max_rot: int = 0, tol: float = 1e-14):
     """Batched reference Jacobi: alpha/beta [chains][ld] -> (lam, w0) [chains][ld]."""
     a = np.ascontiguousarray(alpha, dtype=np.float64)
@@ -577,14 +611,20 @@ class SweepResult:
     n_avg: np.ndarray
     e_avg: np.ndarray
     N_sector: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    # batched method with check > 0: estimated rounding errors against the complex128 path
+    lnz_sector_err: Optional[np.ndarray] = None  # [n_sec][n_T]
+    lnz_gc_err: Optional[np.ndarray] = None  # [n_T][n_mu]
+    n_err: Optional[np.ndarray] = None
 
 
 def grand_canonical_sweep(p: HubbardParams, n_random: int, lanczos_steps: int, seed: int, temperatures, mus,
-                          start: str = "reference", method: str = "plain") -> SweepResult:
+                          start: str = "reference", method: str = "plain", check: int = 0) -> SweepResult:
     """Every (N_up, N_dn) sector, R chains each, then the (T, mu) grid.
 
     method "plain": complex128, one chain at a time (start "reference" or "philox");
-    method "batched": complex64 block vectors of 32 chains, Philox starts (see ftlm_gpu.h)."""
+    method "batched": complex64 block vectors of 32 chains, Philox starts (see ftlm_gpu.h); with
+    check > 0 the first `check` chains of every sector are rerun in complex128 and the result carries
+    the estimated rounding error of each sector ln Z, of ln Z_GC and of <n>."""
     T = np.ascontiguousarray(np.atleast_1d(temperatures), dtype=np.float64)
     bts = np.ascontiguousarray(1.0 / T)
     mu = np.ascontiguousarray(np.atleast_1d(mus), dtype=np.float64)
@@ -596,7 +636,13 @@ def grand_canonical_sweep(p: HubbardParams, n_random: int, lanczos_steps: int, s
     g2 = np.zeros_like(g1)
     g3 = np.zeros_like(g1)
     outs = [x.ctypes.data_as(C.c_void_p) for x in (lz, es, g1, g2, g3)]
-    if method == "batched":
+    errs = None
+    if method == "batched" and check > 0:
+        errs = (np.zeros((nsec, bts.size)), np.zeros((bts.size, mu.size)), np.zeros((bts.size, mu.size)))
+        call("ftlm_gpu_batched_sweep_checked", C.byref(p._c()), n_random, lanczos_steps, C.c_uint(seed & 0xFFFFFFFF),
+             bts.ctypes.data_as(C.c_void_p), bts.size, mu.ctypes.data_as(C.c_void_p), mu.size, int(check), *outs,
+             *[x.ctypes.data_as(C.c_void_p) for x in errs])
+    elif method == "batched":
         call("ftlm_gpu_batched_sweep", C.byref(p._c()), n_random, lanczos_steps, C.c_uint(seed & 0xFFFFFFFF),
              bts.ctypes.data_as(C.c_void_p), bts.size, mu.ctypes.data_as(C.c_void_p), mu.size, *outs)
     else:
@@ -604,4 +650,7 @@ def grand_canonical_sweep(p: HubbardParams, n_random: int, lanczos_steps: int, s
              START_MODES[start], bts.ctypes.data_as(C.c_void_p), bts.size, mu.ctypes.data_as(C.c_void_p), mu.size,
              *outs)
     N = np.array([nu + nd for nu in range(n + 1) for nd in range(n + 1)])
-    return SweepResult(T, bts, mu, lz, es, g1, g2, g3, N)
+    r = SweepResult(T, bts, mu, lz, es, g1, g2, g3, N)
+    if errs is not None:
+        r.lnz_sector_err, r.lnz_gc_err, r.n_err = errs
+    return r

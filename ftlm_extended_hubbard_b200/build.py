@@ -27,7 +27,7 @@ PYMOD_DIR = os.path.join(HERE, "python", "ftlm")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"] + ARCH
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC"]
-CU_SOURCES = ["hv.cu", "lanczos.cu", "quad.cu", "capi.cu", "capi_batched.cu", "capi_grad.cu", "capi_orbit.cu", "noalloc.cu", "batched.cu", "orbit.cu", "grad.cu", "chains.cu"]
+CU_SOURCES = ["hv.cu", "lanczos.cu", "quad.cu", "capi.cu", "capi_batched.cu", "capi_grad.cu", "capi_orbit.cu", "noalloc.cu", "batched.cu", "orbit.cu", "grad.cu", "chains.cu", "symeig.cu"]
 CXX_SOURCES = ["plan.cpp", "tridiag.cpp"]
 
 

@@ -5,11 +5,11 @@
 // path (plan.hpp), same recurrence as src/lanczos.cpp:180-205, with these changes of form:
 //
 //   * vectors are kept unnormalised: W_k = beta_{k-1} q_k (W_0 = raw start, beta_{-1} = ||raw||),
-//     and the 1/beta_{k-1} factor is applied to the H·v result in the kernel epilogue
-//       Y = H q_k = (H W_k) / beta_{k-1}
-//       z = <q_k, Y> = <W_k, Y> / beta_{k-1},  alpha_k = Re z
-//       W_{k+1} = Y - (z / beta_{k-1}) W_k - (beta_{k-1} / beta_{k-2}) W_{k-1},  beta_k = ||W_{k+1}||
-//     so no normalisation pass exists;
+//     and the 1/beta_{k-1} factor is applied in FP64 after the H·v, never rounded to FP32:
+//       Y = H W_k                              (FP32, unscaled)
+//       z = <q_k, H q_k> = <W_k, Y> / beta_{k-1}^2,  alpha_k = Re z
+//       W_{k+1} = Y / beta_{k-1} - (z / beta_{k-1}) W_k - (beta_{k-1} / beta_{k-2}) W_{k-1},  beta_k = ||W_{k+1}||
+//     so no normalisation pass exists, and no per-step FP32 rounding of the scale enters alpha;
 //   * alpha/beta stay on the device; a chain whose ||w||^2 < 1e-24 stops (reference breakdown
 //     rule) and its later scale factors are 0;
 //   * H·v in FP32 (FMA), dot products and norms accumulated in FP64 with Neumaier compensation,
@@ -88,7 +88,9 @@ __device__ __forceinline__ uint4 philox(uint4 c, uint2 k) {
 }
 
 __global__ void __launch_bounds__(kBtThreads) bt_start_kernel(float2* __restrict__ W, int64_t dim, unsigned seed,
-                                                              double* __restrict__ partial, int* __restrict__ flag) {
+                                                              double* __restrict__ partial, int* __restrict__ flag,
+                                                              const uint32_t* __restrict__ umask,
+                                                              const uint32_t* __restrict__ dmask, int64_t Dd) {
   __shared__ double sh[kBtThreads];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned key = seed + static_cast<unsigned>(lane) * 100003u;
@@ -103,7 +105,11 @@ __global__ void __launch_bounds__(kBtThreads) bt_start_kernel(float2* __restrict
     const double rad = sqrt(-2.0 * log(u1));
     double s, c;
     sincospi(2.0 * u2, &s, &c);
-    const float2 z = make_float2(static_cast<float>(rad * c), static_cast<float>(rad * s));
+    float2 z = make_float2(static_cast<float>(rad * c), static_cast<float>(rad * s));
+    if (umask) {  // the start vector expressed in the gauge basis: W = G r
+      const int64_t r = i / Dd;
+      if (gauge_sign(umask[r], dmask[i - r * Dd])) z = make_float2(-z.x, -z.y);
+    }
     if (tinyf(z) && (z.x != 0.f || z.y != 0.f)) *flag = 1;
     W[i * 32 + lane] = z;
     acc.add(static_cast<double>(z.x) * z.x + static_cast<double>(z.y) * z.y);
@@ -152,14 +158,14 @@ __device__ __forceinline__ float4 fold_halves(float4 a) {
 // division runs per basis state; vector offsets are counted in float4 units (< 2^32 up to a
 // 68 GB block vector).
 
-// Row pass: Y[r, c, :] = s_in * (diag * W + down hops).  Warp-persistent over basis states in
-// row-major order (all warps of the grid walk the same row together, so the row of W —
-// Dd * 256 bytes — is served from L2).  Each warp keeps the down-hop coefficients of its current
-// row with the up-string JW factor folded in; no block barriers.
+// Row pass (gauge basis): Y[r, c, :] = diag * W + down hops.  Warp-persistent over basis states in
+// row-major order (all warps of the grid walk the same row together, so the row of W — Dd * 256
+// bytes — is served from L2).  In the gauge basis the down-hop coefficients do not depend on the
+// up string: entry (2*hop + down-string sign) indexes one global signed table (dn_coef32s).
 template <bool kFilter>
 __device__ __forceinline__ void bt_rows_body(const DevSector& S, const float4* __restrict__ Wrow,
-                                             float4* __restrict__ Yrow, float4 sc, const float2* s_row, uint32_t u,
-                                             int cuu, uint4 wp, int c, int lane) {
+                                             float4* __restrict__ Yrow, uint32_t u, int cuu, uint4 wp, int c,
+                                             int lane) {
   const int hv = lane >> 4;
   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
   if (hv == 0) {
@@ -180,53 +186,32 @@ __device__ __forceinline__ void bt_rows_body(const DevSector& S, const float4* _
 #pragma unroll
     for (int t = 0; t < 4; ++t) v[t] = Wrow[(e[t] >> 9) << 4];
 #pragma unroll
-    for (int t = 0; t < 4; ++t) cmac4(acc, s_row[e[t] & 511u], kFilter ? filt4(v[t]) : v[t], 0u);
+    for (int t = 0; t < 4; ++t) cmac4(acc, __ldg(S.dn_coef32s + (e[t] & 511u)), kFilter ? filt4(v[t]) : v[t], 0u);
   }
   acc = fold_halves(acc);
-  if (hv == 0)
-    Yrow[static_cast<uint32_t>(c) * 16u] = make_float4(acc.x * sc.x, acc.y * sc.x, acc.z * sc.z, acc.w * sc.z);
+  if (hv == 0) Yrow[static_cast<uint32_t>(c) * 16u] = acc;
 }
 
 __global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_rows_kernel(DevSector S, const float2* __restrict__ W,
                                                                              float2* __restrict__ Y,
-                                                                             const double* __restrict__ st,
                                                                              const int* __restrict__ flag) {
-  __shared__ float2 s_row[kBtWarps][512];  // [2*hop + down-string sign], up-string sign folded in
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int l = lane & 15;
-  const float4 sc = make_float4(static_cast<float>(st[kBtSin * 32 + 2 * l]), 0.f,
-                                static_cast<float>(st[kBtSin * 32 + 2 * l + 1]), 0.f);
   const bool filter = *flag != 0;
   const int Dd = static_cast<int>(S.Dd), Du = static_cast<int>(S.Du);
   const int gw = blockIdx.x * kBtWarps + warp;
   const int nw = gridDim.x * kBtWarps;
-  float2* tab = s_row[warp];
   int r = gw / Dd, c = gw - (gw / Dd) * Dd;
-  int cur_row = -1;
-  uint32_t u = 0;
-  int cuu = 0;
-  uint4 wp = make_uint4(0, 0, 0, 0);
   while (r < Du) {
-    if (r != cur_row) {
-      __syncwarp();
-      u = S.umask[r];
-      cuu = S.cnt_uu[r];
-      wp = S.wpl[r];
-      for (int i = lane; i < 2 * (S.n_dn_hops + 1); i += 32) {
-        const int h = i >> 1;
-        const float2 cf = S.dn_coef32[h];
-        const float sg = ((__popc(u & S.dn_nmask[h]) ^ i) & 1) ? -1.f : 1.f;
-        tab[i] = make_float2(sg * cf.x, sg * cf.y);
-      }
-      __syncwarp();
-      cur_row = r;
-    }
+    const uint32_t u = S.umask[r];
+    const int cuu = S.cnt_uu[r];
+    const uint4 wp = S.wpl[r];
     const float4* Wrow = reinterpret_cast<const float4*>(W) + static_cast<int64_t>(r) * Dd * 16 + l;
     float4* Yrow = reinterpret_cast<float4*>(Y) + static_cast<int64_t>(r) * Dd * 16 + l;
     if (filter)
-      bt_rows_body<true>(S, Wrow, Yrow, sc, tab, u, cuu, wp, c, lane);
+      bt_rows_body<true>(S, Wrow, Yrow, u, cuu, wp, c, lane);
     else
-      bt_rows_body<false>(S, Wrow, Yrow, sc, tab, u, cuu, wp, c, lane);
+      bt_rows_body<false>(S, Wrow, Yrow, u, cuu, wp, c, lane);
     c += nw;
     while (c >= Dd) {
       c -= Dd;
@@ -235,11 +220,7 @@ __global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_rows_kernel(Dev
   }
 }
 
-// Column pass: Y[r, c, :] += s_in * sum_j coef_j s_j(c) W[src_j, c, :], then the fused dot
-// <W_k, Y> per chain.  Warp-persistent over basis states in column-major order (the grid walks
-// one column of W at a time: Du * 256 bytes in L2).  Each warp builds its state's signed
-// coefficient list (padded to a multiple of 8 with zero coefficients) in its own shared-memory
-// slot; block barriers only for the final dot sums.
+// Gathers of the orbit pass: two half-warps take every other source of the warp's list.
 template <bool kFilter>
 __device__ __forceinline__ float4 bt_cols_sum(const float4* Wc, const uint32_t* s_off, const float2* s_cf, int deg8,
                                               int hv) {
@@ -254,57 +235,72 @@ __device__ __forceinline__ float4 bt_cols_sum(const float4* Wc, const uint32_t* 
   return fold_halves(acc);
 }
 
+// Column pass (gauge basis): Y[r, c, :] += sum_j u_j W[src_j, c, :] with the coefficients u_j of
+// output up string r the same for every column (the down string no longer enters the sign), then
+// the fused <W_k, Y> per chain.  Work item = (16-column chunk, output row r), walked chunk-major by
+// a persistent grid so that the chunk's slab of W (Du x 16 x 256 bytes) stays in L2; in an item,
+// thread (column t/16, lane t%16) owns chains 2l, 2l+1 of one column and every source row is read
+// as one contiguous 4-kilobyte segment.  Each block keeps its items' dot sums in registers and
+// writes one partial per chain (fixed work order: bitwise repeatable).
+constexpr int kBgCols = 16;
+
+template <bool kFilter>
+__device__ __forceinline__ float4 bg_cols_sum(const float4* __restrict__ Wc, const uint32_t* s_off,
+                                              const float2* s_cf, int deg) {
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  int j = 0;
+  for (; j + 4 <= deg; j += 4) {
+    float4 v[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) v[t] = Wc[s_off[j + t]];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) cmac4(acc, s_cf[j + t], kFilter ? filt4(v[t]) : v[t], 0u);
+  }
+  for (; j < deg; ++j) {
+    const float4 v = Wc[s_off[j]];
+    cmac4(acc, s_cf[j], kFilter ? filt4(v) : v, 0u);
+  }
+  return acc;
+}
+
 __global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_cols_kernel(DevSector S, const float2* __restrict__ W,
                                                                              float2* __restrict__ Y,
-                                                                             const double* __restrict__ st,
                                                                              double* __restrict__ partial,
                                                                              const int* __restrict__ flag) {
-  __shared__ uint32_t s_off[kBtWarps][kMaxUpDegB];
-  __shared__ float2 s_cf[kBtWarps][kMaxUpDegB];
+  __shared__ uint32_t s_off[kMaxUpDegB];
+  __shared__ float2 s_cf[kMaxUpDegB];
   __shared__ double sh[4 * kBtThreads];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int hv = lane >> 4, l = lane & 15;
-  const float4 sc = make_float4(static_cast<float>(st[kBtSin * 32 + 2 * l]), 0.f,
-                                static_cast<float>(st[kBtSin * 32 + 2 * l + 1]), 0.f);
+  const int t = threadIdx.x;
+  const int col = t >> 4, l = t & 15;
   const bool filter = *flag != 0;
   const int Dd = static_cast<int>(S.Dd), Du = static_cast<int>(S.Du);
   const uint32_t row_stride = static_cast<uint32_t>(Dd) * 16u;  // float4 units per row
   const float4* W4 = reinterpret_cast<const float4*>(W);
   float4* Y4 = reinterpret_cast<float4*>(Y);
-  const int gw = blockIdx.x * kBtWarps + warp;
-  const int nw = gridDim.x * kBtWarps;
-  uint32_t* off = s_off[warp];
-  float2* cfs = s_cf[warp];
-  double d0r = 0.0, d0i = 0.0, d1r = 0.0, d1i = 0.0;  // chains 2l and 2l+1 (half-warp 0 only)
-  int c = gw / Du, r = gw - (gw / Du) * Du;  // column-major walk
-  while (c < Dd) {
+  const int64_t nchunks = (Dd + kBgCols - 1) / kBgCols;
+  const int64_t items = nchunks * Du;
+  double d0r = 0.0, d0i = 0.0, d1r = 0.0, d1i = 0.0;  // chains 2l and 2l+1
+  for (int64_t it = blockIdx.x; it < items; it += gridDim.x) {
+    const int64_t chunk = it / Du;
+    const int r = static_cast<int>(it - chunk * Du);
     const int j0 = S.up_ptr[r];
     const int deg = S.up_ptr[r + 1] - j0;
-    const uint32_t q = prefix_parity_shifted(S.dmask[c]);
-    const int deg8 = (deg + 7) & ~7;
-    __syncwarp();
-    for (int j = lane; j < deg8; j += 32) {
-      if (j < deg) {
-        off[j] = static_cast<uint32_t>(S.up_src[j0 + j]) * row_stride;
-        const uint32_t lh = S.up_lohi[j0 + j];
-        const uint32_t f = (((q >> (lh & 255u)) ^ (q >> (lh >> 8))) & 1u) << 31;
-        const float2 cd = S.up_coef32[j0 + j];
-        cfs[j] = make_float2(__uint_as_float(__float_as_uint(cd.x) ^ f), __uint_as_float(__float_as_uint(cd.y) ^ f));
-      } else {  // padding: a valid address, zero coefficient
-        off[j] = static_cast<uint32_t>(r) * row_stride;
-        cfs[j] = make_float2(0.f, 0.f);
-      }
+    __syncthreads();  // the previous item's list is no longer read
+    for (int j = t; j < deg; j += kBtThreads) {
+      s_off[j] = static_cast<uint32_t>(S.up_src[j0 + j]) * row_stride;
+      s_cf[j] = S.up_coef32[j0 + j];
     }
-    __syncwarp();
-    const float4* Wc = W4 + static_cast<uint32_t>(c) * 16u + l;
-    const float4 acc = filter ? bt_cols_sum<true>(Wc, off, cfs, deg8, hv) : bt_cols_sum<false>(Wc, off, cfs, deg8, hv);
-    if (hv == 0) {
+    __syncthreads();
+    const int c = static_cast<int>(chunk) * kBgCols + col;
+    if (c < Dd) {
+      const float4* Wc = W4 + static_cast<uint32_t>(c) * 16u + l;
+      const float4 acc = filter ? bg_cols_sum<true>(Wc, s_off, s_cf, deg) : bg_cols_sum<false>(Wc, s_off, s_cf, deg);
       const int64_t o = static_cast<int64_t>(r) * row_stride + static_cast<uint32_t>(c) * 16u + l;
       float4 y = Y4[o];
-      y.x = fmaf(acc.x, sc.x, y.x);
-      y.y = fmaf(acc.y, sc.x, y.y);
-      y.z = fmaf(acc.z, sc.z, y.z);
-      y.w = fmaf(acc.w, sc.z, y.w);
+      y.x += acc.x;
+      y.y += acc.y;
+      y.z += acc.z;
+      y.w += acc.w;
       Y4[o] = y;
       const float4 w = W4[o];
       // conj(w) * y per chain
@@ -315,14 +311,8 @@ __global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_cols_kernel(Dev
       d1r = fma(wz, yz, fma(ww, yw, d1r));
       d1i = fma(wz, yw, fma(-ww, yz, d1i));
     }
-    r += nw;
-    while (r >= Du) {
-      r -= Du;
-      ++c;
-    }
   }
-  // per-chain block sums: lane l of every warp holds chains 2l, 2l+1
-  const int t = threadIdx.x;
+  // per-chain block sums: thread t holds chains 2l, 2l+1 of column t/16
   sh[0 * kBtThreads + t] = d0r;
   sh[1 * kBtThreads + t] = d0i;
   sh[2 * kBtThreads + t] = d1r;
@@ -331,9 +321,9 @@ __global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_cols_kernel(Dev
   if (t < 32) {
     const int ll = t & 15, which = t >> 4;  // thread t reduces chain 2*ll + which
     double re = 0.0, im = 0.0;
-    for (int w = 0; w < kBtWarps; ++w) {
-      re += sh[(2 * which) * kBtThreads + w * 32 + ll];
-      im += sh[(2 * which + 1) * kBtThreads + w * 32 + ll];
+    for (int k = 0; k < kBtThreads / 16; ++k) {
+      re += sh[(2 * which) * kBtThreads + k * 16 + ll];
+      im += sh[(2 * which + 1) * kBtThreads + k * 16 + ll];
     }
     const int chain = 2 * ll + which;
     partial[(blockIdx.x * 32 + chain) * 2] = re;
@@ -341,7 +331,7 @@ __global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_cols_kernel(Dev
   }
 }
 
-// W_{k+1} = Y - c1 W_k - c2 W_{k-1} (in Y's buffer), ||W_{k+1}||^2 partials per chain.
+// W_{k+1} = s_in Y - c1 W_k - c2 W_{k-1} (in Y's buffer, FP64 then rounded), ||W_{k+1}||^2 partials per chain.
 __global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_update_kernel(float2* __restrict__ Y,
                                                                                const float2* __restrict__ Wk,
                                                                                const float2* __restrict__ Wkm1,
@@ -350,6 +340,7 @@ __global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_update_kernel(f
                                                                                int* __restrict__ flag) {
   __shared__ double sh[kBtThreads];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const double s_in = st[kBtSin * 32 + lane];
   const double c1r = st[kBtC1r * 32 + lane], c1i = st[kBtC1i * 32 + lane];
   const double c2 = use_prev ? st[kBtC2 * 32 + lane] : 0.0;
   Neu acc;
@@ -368,8 +359,8 @@ __global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_update_kernel(f
     for (int t = 0; t < 4; ++t) {
       const int64_t i = i0 + t * stride;
       if (i >= dim) continue;
-      double wr = static_cast<double>(y[t].x) - (c1r * a[t].x - c1i * a[t].y);
-      double wi = static_cast<double>(y[t].y) - (c1r * a[t].y + c1i * a[t].x);
+      double wr = s_in * static_cast<double>(y[t].x) - (c1r * a[t].x - c1i * a[t].y);
+      double wi = s_in * static_cast<double>(y[t].y) - (c1r * a[t].y + c1i * a[t].x);
       wr -= c2 * b[t].x;
       wi -= c2 * b[t].y;
       const float2 w = make_float2(static_cast<float>(wr), static_cast<float>(wi));
@@ -384,7 +375,7 @@ __global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_update_kernel(f
 }
 
 // One warp: chain lane.  mode 0: start norms -> s_in = 1/||raw||, c2 = 0.
-// mode 1: dot partials -> z, alpha_k, c1 = z * s_in.  mode 2: norm partials -> beta_k, next
+// mode 1: dot partials <W_k, H W_k> -> z = s_in^2 <W_k, H W_k>, alpha_k, c1 = z * s_in.  mode 2: norm partials -> beta_k, next
 // s_in = 1/beta_k, c2 = beta_k * s_in (old), breakdown bookkeeping.
 __global__ void bt_scalar_kernel(const double* __restrict__ partial, int nblocks, int mode, int k,
                                  double* __restrict__ st, double* __restrict__ alpha, double* __restrict__ beta,
@@ -398,7 +389,7 @@ __global__ void bt_scalar_kernel(const double* __restrict__ partial, int nblocks
       si.add(partial[(b * 32 + lane) * 2 + 1]);
     }
     const double s_in = st[kBtSin * 32 + lane];
-    const double zr = sr.value() * s_in, zi = si.value() * s_in;
+    const double zr = sr.value() * s_in * s_in, zi = si.value() * s_in * s_in;
     st[kBtC1r * 32 + lane] = zr * s_in;
     st[kBtC1i * 32 + lane] = zi * s_in;
     if (st[kBtActive * 32 + lane] != 0.0) alpha[k * 32 + lane] = zr;
@@ -435,7 +426,7 @@ __global__ void bt_scalar_kernel(const double* __restrict__ partial, int nblocks
   st[kBtSin * 32 + lane] = 1.0 / b;
 }
 
-// Orbit momentum block, 32 chains: Y[a, :] = s_in * H_K W[a, :] (complex64 block vectors over the
+// Orbit momentum block, 32 chains: Y[a, :] = H_K W[a, :] (complex64 block vectors over the
 // block's representatives) and the fused <W_k, Y> per chain.  Warp per representative: the lanes
 // walk the representative's sources in the sector's gather tables 32 at a time (table lookup and
 // coefficient <rep a|H|s> eta conj(chi(R)) sqrt|A_b| / sqrt|A_a| in FP64, rounded to complex64) and
@@ -470,8 +461,6 @@ __global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_orbit_kernel(Or
   __shared__ double sh[4 * kBtThreads];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int hv = lane >> 4, l = lane & 15;
-  const float4 sc = make_float4(static_cast<float>(st[kBtSin * 32 + 2 * l]), 0.f,
-                                static_cast<float>(st[kBtSin * 32 + 2 * l + 1]), 0.f);
   const bool filter = *flag != 0;
   const DevSector& S = A.S;
   const int64_t Dd = S.Dd;
@@ -545,10 +534,10 @@ __global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_orbit_kernel(Or
       const float4 wf = filter ? filt4(w) : w;
       const float dg = static_cast<float>(diag_value(S, u, d, S.cnt_uu[ru], S.cnt_dd[rd], S.wpl[ru]));
       float4 y;
-      y.x = (acc.x + dg * wf.x) * sc.x;
-      y.y = (acc.y + dg * wf.y) * sc.x;
-      y.z = (acc.z + dg * wf.z) * sc.z;
-      y.w = (acc.w + dg * wf.w) * sc.z;
+      y.x = acc.x + dg * wf.x;
+      y.y = acc.y + dg * wf.y;
+      y.z = acc.z + dg * wf.z;
+      y.w = acc.w + dg * wf.w;
       Y4[static_cast<uint32_t>(a) * 16u + l] = y;
       const double wx = w.x, wy = w.y, wz = w.z, ww = w.w;
       const double yx = y.x, yy = y.y, yz = y.z, yw = y.w;
@@ -580,10 +569,11 @@ __global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_orbit_kernel(Or
 }  // namespace
 
 cudaError_t bt_start(float2* W, int64_t dim, unsigned seed, double* st, double* partial, int* used, int* flags,
-                     cudaStream_t s) {
+                     cudaStream_t s, const DevSector* gauge) {
   cudaError_t e = cudaMemsetAsync(flags, 0, 2 * sizeof(int), s);
   if (e != cudaSuccess) return e;
-  bt_start_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(W, dim, seed, partial, flags);
+  bt_start_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(W, dim, seed, partial, flags, gauge ? gauge->umask : nullptr,
+                                                   gauge ? gauge->dmask : nullptr, gauge ? gauge->Dd : 1);
   bt_scalar_kernel<<<1, 32, 0, s>>>(partial, kBtBlocks, 0, 0, st, nullptr, nullptr, used);
   return cudaGetLastError();
 }
@@ -595,8 +585,8 @@ cudaError_t bt_step(const DevSector& S, const float2* Wk, const float2* Wkm1, fl
   int* fout = flags + ((k + 1) & 1);
   cudaError_t e = cudaMemsetAsync(fout, 0, sizeof(int), s);
   if (e != cudaSuccess) return e;
-  bt_rows_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(S, Wk, Y, st, fin);
-  bt_cols_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(S, Wk, Y, st, partial, fin);
+  bt_rows_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(S, Wk, Y, fin);
+  bt_cols_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(S, Wk, Y, partial, fin);
   bt_scalar_kernel<<<1, 32, 0, s>>>(partial, kBtBlocks, 1, k, st, alpha, beta, used);
   bt_update_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(Y, Wk, Wkm1, S.dim, st, k > 0, partial, fout);
   bt_scalar_kernel<<<1, 32, 0, s>>>(partial, kBtBlocks, 2, k, st, alpha, beta, used);
@@ -618,8 +608,9 @@ cudaError_t bt_orbit_step(const OrbitApplyDev& A, const float2* Wk, const float2
 
 cudaError_t bt_apply(const DevSector& S, const float2* X, float2* Y, const double* st_unit, double* partial,
                      const int* zero_flag, cudaStream_t s) {
-  bt_rows_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(S, X, Y, st_unit, zero_flag);
-  bt_cols_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(S, X, Y, st_unit, partial, zero_flag);
+  (void)st_unit;
+  bt_rows_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(S, X, Y, zero_flag);
+  bt_cols_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(S, X, Y, partial, zero_flag);
   return cudaGetLastError();
 }
 

@@ -21,10 +21,14 @@ constexpr int kBtFields = 8;
 constexpr int kBtPartialDoubles = kBtBlocks * kBtChains * 2;
 
 // W <- complex64 Philox start vectors (chain r: key seed + r*100003), norms -> scalar state.
-// flags: 2 ints (tiny-entry flags of the current and next vector, cleared here).
+// flags: 2 ints (tiny-entry flags of the current and next vector, cleared here).  gauge: the sector
+// whose spin-ordered basis the block vectors of bt_step live in (the start vector G r, G the
+// diagonal sign matrix of gauge_sign); null for orbit blocks (their own basis).
 cudaError_t bt_start(float2* W, int64_t dim, unsigned seed, double* st, double* partial, int* used, int* flags,
-                     cudaStream_t s);
-// One Lanczos step k for all chains: Y <- H q_k, z, W_{k+1} (into Y), beta_k; alpha/beta [M][32].
+                     cudaStream_t s, const DevSector* gauge);
+// One Lanczos step k for all chains on block vectors in the sector's gauge basis (bt_start with
+// gauge = &S): Y <- H W_k, z, W_{k+1} (into Y), beta_k; alpha/beta [M][32].  G H G has the same
+// spectrum and the start vectors are G r, so alpha/beta are those of the original basis.
 cudaError_t bt_step(const DevSector& S, const float2* Wk, const float2* Wkm1, float2* Y, int k, double* st,
                     double* partial, double* alpha, double* beta, int* used, int* flags, cudaStream_t s);
 
@@ -34,8 +38,8 @@ cudaError_t bt_step(const DevSector& S, const float2* Wk, const float2* Wkm1, fl
 cudaError_t bt_orbit_step(const OrbitApplyDev& A, const float2* Wk, const float2* Wkm1, float2* Y, int k, double* st,
                           double* partial, double* alpha, double* beta, int* used, int* flags, cudaStream_t s);
 
-// Y = H X for one block vector, without Lanczos bookkeeping: st_unit holds kBtSin = 1 for every
-// chain, zero_flag points to an int 0 (no small-entry filter), partial receives unused dot sums.
+// Y = (G H G) X for one block vector in the gauge basis, without Lanczos bookkeeping (st_unit is
+// unused), zero_flag points to an int 0 (no small-entry filter), partial receives unused dot sums.
 cudaError_t bt_apply(const DevSector& S, const float2* X, float2* Y, const double* st_unit, double* partial,
                      const int* zero_flag, cudaStream_t s);
 

@@ -6,11 +6,16 @@
 #include <map>
 #include <thread>
 
+#include <atomic>
+
 #include "capi_internal.hpp"
 #include "chains.cuh"
 
 using namespace ftlm_b200;
 using namespace ftlm_b200::capi;
+
+// Quadrature of the complex128 sector path (ftlm_gpu_set_quadrature).
+static std::atomic<bool> g_quad_converged{false};
 
 namespace {
 thread_local std::string g_err;
@@ -76,9 +81,15 @@ int upload_plan(ftlm_sector* s) {
     dnc[i] = make_double2(P.dn_coef[2 * i], P.dn_coef[2 * i + 1]);
     dnc32[i] = make_float2(static_cast<float>(dnc[i].x), static_cast<float>(dnc[i].y));
   }
-  float2 *ucf32, *dcf32;
+  std::vector<float2> dnc32s(2 * dnc32.size());
+  for (size_t i = 0; i < dnc32.size(); ++i) {
+    dnc32s[2 * i] = dnc32[i];
+    dnc32s[2 * i + 1] = make_float2(-dnc32[i].x, -dnc32[i].y);
+  }
+  float2 *ucf32, *dcf32, *dcf32s;
   CU_TRY(upload(upc32, &ucf32, &s->owned));
   CU_TRY(upload(dnc32, &dcf32, &s->owned));
+  CU_TRY(upload(dnc32s, &dcf32s, &s->owned));
   uint32_t *um, *dm, *ulh, *dent, *dnm;
   int32_t *cuu, *cdd, *uptr, *usrc;
   uint4* wp;
@@ -104,6 +115,22 @@ int upload_plan(ftlm_sector* s) {
   std::vector<int> flags(4, 0);
   int* fl;
   CU_TRY(upload(flags, &fl, &s->owned));
+  D.dn_ent4 = nullptr;
+  D.dn_gptr4 = nullptr;
+  if (P.dn_compact) {
+    uint32_t* e4;
+    int64_t* g4;
+    CU_TRY(upload(P.dn_ent4, &e4, &s->owned));
+    CU_TRY(upload(P.dn_gptr4, &g4, &s->owned));
+    D.dn_ent4 = reinterpret_cast<const uint4*>(e4);
+    D.dn_gptr4 = g4;
+    for (int i = 0; i < 4; ++i) {
+      D.dn_re[i] = P.dn_re[i];
+      D.dn_im[i] = P.dn_im[i];
+    }
+    D.dn_re_bits = P.dn_re_bits;
+    D.dn_im_bits = P.dn_im_bits;
+  }
   D.umask = um;
   D.dmask = dm;
   D.cnt_uu = cuu;
@@ -118,6 +145,7 @@ int upload_plan(ftlm_sector* s) {
   D.dn_csr_ptr = cptr;
   D.up_coef32 = ucf32;
   D.dn_coef32 = dcf32;
+  D.dn_coef32s = dcf32s;
   D.dn_csr_ent = cent;
   D.dn_coef = dcf;
   D.dn_nmask = dnm;
@@ -273,6 +301,24 @@ int ftlm_gpu_sector_state(const ftlm_sector* s, long long index, uint64_t* up, u
   return FTLM_OK;
 }
 
+int ftlm_gpu_sector_down_table_compact(const ftlm_sector* s, int* available, long long* n_groups,
+                                       long long* n_entries, long long* gptr, uint32_t* entries, double* re4,
+                                       double* im4, int* re_bits, int* im_bits) {
+  if (!s || !available || !n_groups || !n_entries) return fail(FTLM_ERR_INVALID, "null argument");
+  const SectorPlan& P = s->plan;
+  *available = P.dn_compact ? 1 : 0;
+  *n_groups = P.dn_compact ? static_cast<long long>(P.dn_gptr4.size()) - 1 : 0;
+  *n_entries = static_cast<long long>(P.dn_ent4.size());
+  if (!P.dn_compact) return FTLM_OK;
+  if (gptr) std::copy(P.dn_gptr4.begin(), P.dn_gptr4.end(), gptr);
+  if (entries) std::copy(P.dn_ent4.begin(), P.dn_ent4.end(), entries);
+  if (re4) std::copy(P.dn_re, P.dn_re + 4, re4);
+  if (im4) std::copy(P.dn_im, P.dn_im + 4, im4);
+  if (re_bits) *re_bits = P.dn_re_bits;
+  if (im_bits) *im_bits = P.dn_im_bits;
+  return FTLM_OK;
+}
+
 int ftlm_gpu_sector_stats(const ftlm_sector* s, double* mean_up, double* mean_dn, long long* du, long long* dd) {
   if (!s) return fail(FTLM_ERR_INVALID, "null sector");
   if (mean_up) *mean_up = s->plan.mean_up_sources;
@@ -301,7 +347,7 @@ int ftlm_gpu_sector_diag(const ftlm_sector* s, long long index, double* value) {
 }
 
 int ftlm_gpu_set_apply_path(ftlm_sector* s, int path) {
-  if (!s || path < 0 || path > 2) return fail(FTLM_ERR_INVALID, "bad path");
+  if (!s || path < 0 || path > 3) return fail(FTLM_ERR_INVALID, "bad path");
   s->apply_path = path;
   return FTLM_OK;
 }
@@ -321,24 +367,25 @@ int ftlm_gpu_apply_profiled(ftlm_sector* s, const double* x, double* y, void* st
   if (x == y) return fail(FTLM_ERR_INVALID, "x and y must not alias");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int path = s->effective_path();
+  const DevSector d = s->dev_for(path);
   cudaEvent_t ev[3];
   for (auto& e : ev) CU_TRY(cudaEventCreate(&e));
   CU_TRY(cudaEventRecord(ev[0], st));
-  if (path == 2) {
-    CU_TRY(hv_launch_pass(s->dev, reinterpret_cast<const double2*>(x), reinterpret_cast<double2*>(y), 0, st,
+  if (path >= 2) {
+    CU_TRY(hv_launch_pass(d, reinterpret_cast<const double2*>(x), reinterpret_cast<double2*>(y), 0, st,
                           s->cols_variant));
     CU_TRY(cudaEventRecord(ev[1], st));
-    CU_TRY(hv_launch_pass(s->dev, reinterpret_cast<const double2*>(x), reinterpret_cast<double2*>(y), 1, st,
+    CU_TRY(hv_launch_pass(d, reinterpret_cast<const double2*>(x), reinterpret_cast<double2*>(y), 1, st,
                           s->cols_variant));
   } else {
-    CU_TRY(hv_launch(s->dev, reinterpret_cast<const double2*>(x), reinterpret_cast<double2*>(y), path, st));
+    CU_TRY(hv_launch(d, reinterpret_cast<const double2*>(x), reinterpret_cast<double2*>(y), path, st));
     CU_TRY(cudaEventRecord(ev[1], st));
   }
   CU_TRY(cudaEventRecord(ev[2], st));
   CU_TRY(cudaEventSynchronize(ev[2]));
   CU_TRY(cudaEventElapsedTime(&ms_passes[0], ev[0], ev[1]));
   *n_passes = 1;
-  if (path == 2) {
+  if (path >= 2) {
     CU_TRY(cudaEventElapsedTime(&ms_passes[1], ev[1], ev[2]));
     *n_passes = 2;
   }
@@ -363,14 +410,87 @@ int ftlm_gpu_apply_host(ftlm_sector* s, const double* x, double* y) {
   return FTLM_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// The recurrence of src/lanczos.cpp:180-205 on a sector that runs the row + column-slab passes,
+// with the BLAS-1 work folded into them: vectors are kept unnormalised (q_k = s_k W_k, s_k =
+// 1/beta_{k-1}), the row pass stages s_k W_k, the column pass adds s_k times the up-hop sum and
+// emits the partials of z = <q_k, H q_k>, and one pass forms w = H q_k - z q_k - beta_{k-1} q_{k-1}
+// with ||w||^2.  Per step: 8 streaming vector passes instead of 12 and no normalisation pass.
+// alpha and ||w||^2 are read back once per step for the reference's breakdown test.
+int run_lanczos_fused(ftlm_sector* s, int max_steps, unsigned seed, int start_mode, std::vector<double>* alpha,
+                      std::vector<double>* beta) {
+  alpha->clear();
+  beta->clear();
+  const int64_t dim = s->plan.dim;
+  if (dim <= 0 || max_steps <= 0) return FTLM_OK;
+  LanczosWs& ws = s->ws;
+  cudaStream_t st = s->stream;
+  const int path = s->effective_path();
+  const DevSector d = s->dev_for(path);
+  if (hv_rows_smem_bytes(d) > 227 * 1024)
+    return fail(FTLM_ERR_UNSUPPORTED, "row pass does not fit in shared memory for this sector");
+  CU_TRY(ws.ensure(dim));
+  const int64_t nblk = hv_cols_blocks(d, s->cols_variant);
+  CU_TRY(ws.ensure_dotp(nblk));
+  double* scr = ws.scratch.as<double>();
+  if (start_mode == FTLM_START_PHILOX) {
+    CU_TRY(lz_philox_start(ws.q.as<double2>(), dim, seed, scr, st));
+    CU_TRY(lz_normalise_start(ws.q.as<double2>(), dim, scr, st));
+  } else if (start_mode == FTLM_START_REFERENCE) {
+    std::vector<std::complex<double>> h;
+    reference_start(dim, seed, &h);
+    CU_TRY(cudaMemcpyAsync(ws.q.p, h.data(), dim * sizeof(double2), cudaMemcpyHostToDevice, st));
+    CU_TRY(cudaStreamSynchronize(st));
+  } else {
+    return fail(FTLM_ERR_INVALID, "unknown start_mode");
+  }
+  double2* Wk = ws.q.as<double2>();
+  double2* Wkm1 = ws.qp.as<double2>();
+  double2* Y = ws.w.as<double2>();
+  double sk = 1.0, skm1 = 0.0, bprev = 0.0;
+  double res[4];
+  for (int k = 0; k < max_steps; ++k) {
+    CU_TRY(hv_launch_pass(d, Wk, Y, 0, st, s->cols_variant, sk, nullptr));
+    CU_TRY(hv_launch_pass(d, Wk, Y, 1, st, s->cols_variant, sk, ws.dotp.as<double>()));
+    CU_TRY(lz_reduce_pairs(ws.dotp.as<double>(), nblk, scr, st));
+    CU_TRY(lz_update_scaled(Y, Wk, sk, Wkm1, skm1, bprev, k > 0, dim, scr, st));
+    CU_TRY(cudaMemcpyAsync(res, scr + kResZ, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CU_TRY(cudaStreamSynchronize(st));
+    alpha->push_back(res[0]);
+    const double nw2 = res[2];
+    if (nw2 < 1e-24) break;
+    const double b_k = std::sqrt(nw2);
+    beta->push_back(b_k);
+    // rotate: W_{k-1} <- W_k, W_k <- w (unnormalised, scale 1/b_k), the old W_{k-1} buffer is next Y
+    double2* t = Wkm1;
+    Wkm1 = Wk;
+    Wk = Y;
+    Y = t;
+    skm1 = sk;
+    sk = 1.0 / b_k;
+    bprev = b_k;
+  }
+  return FTLM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int ftlm_gpu_lanczos(ftlm_sector* s, int max_steps, unsigned seed, int start_mode, double* alpha, double* beta,
                      int* n_beta, int* used) {
   int rc = need_device(s);
   if (rc) return rc;
   std::vector<double> a, b;
-  rc = run_lanczos(
-      s->plan.dim, [s](const double2* x, double2* y, cudaStream_t st) { return s->apply(x, y, st); }, s->ws,
-      max_steps, seed, start_mode, s->stream, &a, &b);
+  if (s->effective_path() >= 2)
+    rc = run_lanczos_fused(s, max_steps, seed, start_mode, &a, &b);
+  else
+    rc = run_lanczos(
+        s->plan.dim, [s](const double2* x, double2* y, cudaStream_t st) { return s->apply(x, y, st); }, s->ws,
+        max_steps, seed, start_mode, s->stream, &a, &b);
   if (rc) return rc;
   if (alpha) std::copy(a.begin(), a.end(), alpha);
   if (beta) std::copy(b.begin(), b.end(), beta);
@@ -553,8 +673,24 @@ int ftlm_gpu_lanczos_extrema(ftlm_sector* s, int max_steps, unsigned seed, int s
   return FTLM_OK;
 }
 
+int ftlm_gpu_set_quadrature(int mode) {
+  if (mode != FTLM_QUAD_REFERENCE && mode != FTLM_QUAD_CONVERGED) return fail(FTLM_ERR_INVALID, "unknown quadrature");
+  g_quad_converged.store(mode == FTLM_QUAD_CONVERGED);
+  return FTLM_OK;
+}
+
 int ftlm_gpu_ftlm_sector(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed, int start_mode,
                          double* lnz, double* energy) {
+  return plain_sector_ftlm(s, bts, n_bt, R, M, seed, start_mode, plain_quadrature_converged(), lnz, energy);
+}
+
+}  // extern "C"
+
+namespace ftlm_b200 {
+namespace capi {
+
+int plain_sector_ftlm(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed, int start_mode,
+                      bool converged, double* lnz, double* energy) {
   int rc = need_device(s);
   if (rc) return rc;
   if (n_bt < 0 || (n_bt > 0 && (!bts || !lnz || !energy))) return fail(FTLM_ERR_INVALID, "bad arguments");
@@ -584,7 +720,7 @@ int ftlm_gpu_ftlm_sector(ftlm_sector* s, const double* bts, int n_bt, int R, int
     nv[static_cast<size_t>(r)] = used;
   }
   std::vector<double> lq(static_cast<size_t>(R) * n_bt), eq(static_cast<size_t>(R) * n_bt);
-  rc = ftlm_gpu_tridiag_quadrature(A.data(), B.data(), nv.data(), R, M, bts, n_bt, lq.data(), eq.data());
+  rc = chain_quadrature(A.data(), B.data(), nv.data(), R, M, bts, n_bt, lq.data(), eq.data(), converged);
   if (rc) return rc;
   DevBuf dq, de, dn, dz, den;
   CU_TRY(dq.alloc(lq.size() * sizeof(double)));
@@ -601,6 +737,19 @@ int ftlm_gpu_ftlm_sector(ftlm_sector* s, const double* bts, int n_bt, int R, int
   CU_TRY(cudaMemcpy(energy, den.p, n_bt * sizeof(double), cudaMemcpyDeviceToHost));
   return FTLM_OK;
 }
+
+int chain_quadrature(const double* A, const double* B, const int* n, int nc, int ld, const double* bts, int n_bt,
+                     double* lq, double* eq, bool converged) {
+  return converged ? ftlm_gpu_tridiag_quadrature_exact(A, B, n, nc, ld, bts, n_bt, lq, eq)
+                   : ftlm_gpu_tridiag_quadrature(A, B, n, nc, ld, bts, n_bt, lq, eq);
+}
+
+bool plain_quadrature_converged() { return g_quad_converged.load(); }
+
+}  // namespace capi
+}  // namespace ftlm_b200
+
+extern "C" {
 
 int ftlm_gpu_gc_reduce(const double* lnz_s, const double* e_s, const int* N_s, int n_sec, const double* bts, int n_bt,
                        const double* mus, int n_mu, int n_sites, double* lnz_gc, double* n_avg, double* e_avg) {
@@ -744,7 +893,8 @@ int fused_sectors_lanczos(const std::vector<ftlm_sector*>& secs, int R, int M, u
 }
 
 int fused_sectors_ftlm(const std::vector<ftlm_sector*>& secs, const std::vector<int>& out_idx, int R, int M,
-                       unsigned seed, int start_mode, const double* bts, int n_bt, double* lnz_s, double* e_s) {
+                       unsigned seed, int start_mode, const double* bts, int n_bt, double* lnz_s, double* e_s,
+                       bool converged) {
   if (secs.empty()) return FTLM_OK;
   const int ns = static_cast<int>(secs.size());
   const int nc = ns * R;
@@ -753,7 +903,7 @@ int fused_sectors_ftlm(const std::vector<ftlm_sector*>& secs, const std::vector<
   int rc0 = fused_sectors_lanczos(secs, R, M, seed, start_mode, &A, &B, &used);
   if (rc0) return rc0;
   std::vector<double> lq(static_cast<size_t>(nc) * n_bt), eq(static_cast<size_t>(nc) * n_bt);
-  int rc = ftlm_gpu_tridiag_quadrature(A.data(), B.data(), used.data(), nc, M, bts, n_bt, lq.data(), eq.data());
+  int rc = chain_quadrature(A.data(), B.data(), used.data(), nc, M, bts, n_bt, lq.data(), eq.data(), converged);
   if (rc) return rc;
   for (int i = 0; i < ns; ++i) {
     const size_t o = static_cast<size_t>(i) * R;
@@ -831,14 +981,17 @@ int ftlm_gpu_autotune_apply(ftlm_sector* s, int reps, int* path, int* cols_varia
   CU_TRY(cudaEventCreate(&e1));
   int best_p = 1, best_v = 0;
   float best = 3.4e38f;
-  const bool fast = hv_fast_path_ok(s->dev, P.max_up_deg) && hv_rows_smem_bytes(s->dev) <= 227 * 1024;
-  const int variants[4][2] = {{1, 0}, {2, 0}, {2, 1}, {2, 2}};
+  const bool fast = hv_fast_path_ok(s->dev_for(2), P.max_up_deg);
+  const int variants[5][2] = {{1, 0}, {2, 0}, {2, 1}, {2, 2}, {3, 0}};
   cudaError_t ce = cudaSuccess;
   for (const auto& v : variants) {
-    if (v[0] == 2 && !fast) continue;
-    ce = hv_launch(s->dev, x.as<double2>(), y.as<double2>(), v[0], st, v[1]);  // warm-up
+    if (v[0] >= 2 && !fast) continue;
+    if (v[0] == 3 && (!s->dev.dn_ent4 || hv_rows_smem_bytes(s->dev_for(3)) > 227 * 1024)) continue;
+    const DevSector d = s->dev_for(v[0]);
+    const int lp = v[0] == 3 ? 2 : v[0];
+    ce = hv_launch(d, x.as<double2>(), y.as<double2>(), lp, st, v[1]);  // warm-up
     if (ce == cudaSuccess) ce = cudaEventRecord(e0, st);
-    for (int r = 0; r < reps && ce == cudaSuccess; ++r) ce = hv_launch(s->dev, x.as<double2>(), y.as<double2>(), v[0], st, v[1]);
+    for (int r = 0; r < reps && ce == cudaSuccess; ++r) ce = hv_launch(d, x.as<double2>(), y.as<double2>(), lp, st, v[1]);
     if (ce == cudaSuccess) ce = cudaEventRecord(e1, st);
     if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
     float t = 0.0f;
@@ -904,7 +1057,7 @@ int ftlm_gpu_gc_sweep(const ftlm_params* p, int R, int M, unsigned seed, int sta
       if (rc) return clear_and(small, rc);
     }
   const int rcf = fused_sectors_ftlm(small, small_idx, std::max(1, R), std::max(1, M), seed, start_mode, bts, n_bt,
-                                     lnz_s, e_s);
+                                     lnz_s, e_s, plain_quadrature_converged());
   clear_and(small, FTLM_OK);
   if (rcf) return rcf;
   if (lnz_gc && n_avg && e_avg)

@@ -20,7 +20,7 @@ int bt_run_chains(ftlm_sector* s, int R, int M, unsigned seed, std::vector<doubl
       s->plan.dim, st,
       [&S, st](const float2* wk, const float2* wkm1, float2* y, int k, double* sd, double* part, double* al, double* be,
                int* us, int* fl) { return bt_step(S, wk, wkm1, y, k, sd, part, al, be, us, fl, st); },
-      R, M, seed, A, B, used);
+      R, M, seed, A, B, used, &S);
 }
 
 }  // namespace capi
@@ -44,18 +44,27 @@ int ftlm_gpu_batched_lanczos(ftlm_sector* s, int R, int M, unsigned seed, double
   return FTLM_OK;
 }
 
-int ftlm_gpu_batched_ftlm_sector(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed, double* lnz,
-                                 double* energy) {
+namespace {
+
+// The batched sector estimate, and (n_check > 0) its rounding-error estimate against complex128:
+// chains r < n_check are rerun with complex128 vectors from the same Philox start, and
+// lnz_err[b] = max_r |L_r(c64) - L_r(c128)| over them, L_r the chain's log quadrature at bts[b].
+// Since ln Z_s = ln dim + log mean_r e^{L_r}, a common bound d on |dL_r| bounds |d ln Z_s| by d.
+int batched_sector(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed, int n_check, double* lnz,
+                   double* energy, double* lnz_err) {
   int rc = need_device(s);
   if (rc) return rc;
-  if (n_bt < 0 || (n_bt > 0 && (!bts || !lnz || !energy))) return fail(FTLM_ERR_INVALID, "bad arguments");
+  if (n_bt < 0 || (n_bt > 0 && (!bts || !lnz || !energy)) || (n_check > 0 && n_bt > 0 && !lnz_err))
+    return fail(FTLM_ERR_INVALID, "bad arguments");
   R = std::max(1, R);
   M = std::max(1, M);
   if (M > 160) return fail(FTLM_ERR_UNSUPPORTED, "more than 160 Lanczos steps for the on-chip Jacobi");
   const int64_t dim = s->plan.dim;
+  if (lnz_err) std::fill(lnz_err, lnz_err + n_bt, 0.0);
   // Sectors whose Krylov space the chain can exhaust stay on the complex128 path (same Philox
-  // start vectors), where the reference's breakdown test is meaningful.
-  if (dim <= 2 * static_cast<int64_t>(M)) return ftlm_gpu_ftlm_sector(s, bts, n_bt, R, M, seed, FTLM_START_PHILOX, lnz, energy);
+  // start vectors), where the reference's breakdown test is meaningful; their error is zero.
+  if (dim <= 2 * static_cast<int64_t>(M))
+    return plain_sector_ftlm(s, bts, n_bt, R, M, seed, FTLM_START_PHILOX, true, lnz, energy);
   if (s->plan.max_up_deg > 120)
     return fail(FTLM_ERR_UNSUPPORTED, "batched path: more than 120 up-hop sources per string");
   std::vector<double> A, B;
@@ -63,14 +72,93 @@ int ftlm_gpu_batched_ftlm_sector(ftlm_sector* s, const double* bts, int n_bt, in
   rc = bt_run_chains(s, R, M, seed, &A, &B, &used);
   if (rc) return rc;
   std::vector<double> lq(static_cast<size_t>(R) * n_bt), eq(static_cast<size_t>(R) * n_bt);
-  rc = ftlm_gpu_tridiag_quadrature(A.data(), B.data(), used.data(), R, M, bts, n_bt, lq.data(), eq.data());
+  rc = chain_quadrature(A.data(), B.data(), used.data(), R, M, bts, n_bt, lq.data(), eq.data(), true);
   if (rc) return rc;
-  return ftlm_gpu_ftlm_combine(lq.data(), eq.data(), used.data(), R, n_bt, std::log(static_cast<double>(dim)), lnz, energy);
+  rc = ftlm_gpu_ftlm_combine(lq.data(), eq.data(), used.data(), R, n_bt, std::log(static_cast<double>(dim)), lnz, energy);
+  if (rc || n_check <= 0 || n_bt == 0) return rc;
+  const int nc = std::min(n_check, R);
+  std::vector<double> a(static_cast<size_t>(M), 0.0), b(static_cast<size_t>(M), 0.0), q1(static_cast<size_t>(n_bt)),
+      e1(static_cast<size_t>(n_bt));
+  for (int r = 0; r < nc; ++r) {
+    std::fill(a.begin(), a.end(), 0.0);
+    std::fill(b.begin(), b.end(), 0.0);
+    int nb = 0, u = 0;
+    rc = ftlm_gpu_lanczos(s, M, seed + static_cast<unsigned>(r) * 100003u, FTLM_START_PHILOX, a.data(), b.data(), &nb, &u);
+    if (rc) return rc;
+    rc = chain_quadrature(a.data(), b.data(), &u, 1, M, bts, n_bt, q1.data(), e1.data(), true);
+    if (rc) return rc;
+    for (int k = 0; k < n_bt; ++k) {
+      const double d = std::fabs(lq[static_cast<size_t>(r) * n_bt + k] - q1[static_cast<size_t>(k)]);
+      lnz_err[k] = std::max(lnz_err[k], std::isfinite(d) ? d : std::numeric_limits<double>::infinity());
+    }
+  }
+  return FTLM_OK;
 }
+
+}  // namespace
+
+int ftlm_gpu_batched_ftlm_sector(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed, double* lnz,
+                                 double* energy) {
+  return batched_sector(s, bts, n_bt, R, M, seed, 0, lnz, energy, nullptr);
+}
+
+int ftlm_gpu_batched_ftlm_sector_checked(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed,
+                                         int n_check, double* lnz, double* energy, double* lnz_err) {
+  if (n_check < 1) return fail(FTLM_ERR_INVALID, "n_check must be >= 1");
+  return batched_sector(s, bts, n_bt, R, M, seed, n_check, lnz, energy, lnz_err);
+}
+
+namespace {
+
+int batched_sweep(const ftlm_params* p, int R, int M, unsigned seed, const double* bts, int n_bt, const double* mus,
+                  int n_mu, int n_check, double* lnz_s, double* e_s, double* lnz_gc, double* n_avg, double* e_avg,
+                  double* lnz_s_err);
+
+}  // namespace
 
 int ftlm_gpu_batched_sweep(const ftlm_params* p, int R, int M, unsigned seed, const double* bts, int n_bt,
                            const double* mus, int n_mu, double* lnz_s, double* e_s, double* lnz_gc, double* n_avg,
                            double* e_avg) {
+  return batched_sweep(p, R, M, seed, bts, n_bt, mus, n_mu, 0, lnz_s, e_s, lnz_gc, n_avg, e_avg, nullptr);
+}
+
+int ftlm_gpu_batched_sweep_checked(const ftlm_params* p, int R, int M, unsigned seed, const double* bts, int n_bt,
+                                   const double* mus, int n_mu, int n_check, double* lnz_s, double* e_s, double* lnz_gc,
+                                   double* n_avg, double* e_avg, double* lnz_s_err, double* lnz_gc_err,
+                                   double* n_err) {
+  if (n_check < 1) return fail(FTLM_ERR_INVALID, "n_check must be >= 1");
+  if (!p || !lnz_s_err || !lnz_gc || !n_avg || !e_avg || !lnz_gc_err || !n_err)
+    return fail(FTLM_ERR_INVALID, "null argument");
+  int rc = batched_sweep(p, R, M, seed, bts, n_bt, mus, n_mu, n_check, lnz_s, e_s, lnz_gc, n_avg, e_avg, lnz_s_err);
+  if (rc) return rc;
+  // First-order propagation of the sector errors through the grand-canonical combination:
+  // d ln Z_GC = sum_s w_s d ln Z_s and d<n> = sum_s w_s (N_s/n - <n>) d ln Z_s.
+  const int n = p->Lx * p->Ly;
+  for (int b = 0; b < n_bt; ++b)
+    for (int m = 0; m < n_mu; ++m) {
+      const size_t o = static_cast<size_t>(b) * n_mu + m;
+      double eg = 0.0, en = 0.0;
+      for (int nu = 0; nu <= n; ++nu)
+        for (int nd = 0; nd <= n; ++nd) {
+          const size_t sidx = static_cast<size_t>(nu * (n + 1) + nd);
+          const double lz = lnz_s[sidx * n_bt + b];
+          if (!std::isfinite(lz)) continue;
+          const double w = std::exp(lz + bts[b] * mus[m] * static_cast<double>(nu + nd) - lnz_gc[o]);
+          const double d = lnz_s_err[sidx * n_bt + b];
+          eg += w * d;
+          en += w * std::fabs(static_cast<double>(nu + nd) / n - n_avg[o]) * d;
+        }
+      lnz_gc_err[o] = eg;
+      n_err[o] = en;
+    }
+  return FTLM_OK;
+}
+
+namespace {
+
+int batched_sweep(const ftlm_params* p, int R, int M, unsigned seed, const double* bts, int n_bt, const double* mus,
+                  int n_mu, int n_check, double* lnz_s, double* e_s, double* lnz_gc, double* n_avg, double* e_avg,
+                  double* lnz_s_err) {
   if (!p || !lnz_s || !e_s) return fail(FTLM_ERR_INVALID, "null argument");
   const int n = p->Lx * p->Ly;
   if (n <= 0 || n > 32) return fail(FTLM_ERR_INVALID, "FockBasis: require 1 <= n_sites <= 32 (bit packing)");
@@ -96,19 +184,24 @@ int ftlm_gpu_batched_sweep(const ftlm_params* p, int R, int M, unsigned seed, co
         small_idx.push_back(idx);
         continue;
       }
-      rc = ftlm_gpu_batched_ftlm_sector(s, bts, n_bt, R, M, seed, lnz_s + static_cast<size_t>(idx) * n_bt,
-                                        e_s + static_cast<size_t>(idx) * n_bt);
+      rc = batched_sector(s, bts, n_bt, R, M, seed, n_check, lnz_s + static_cast<size_t>(idx) * n_bt,
+                          e_s + static_cast<size_t>(idx) * n_bt,
+                          lnz_s_err ? lnz_s_err + static_cast<size_t>(idx) * n_bt : nullptr);
       ftlm_gpu_sector_destroy(s);
       if (rc) return clear_and(rc);
     }
   const int rcf = fused_sectors_ftlm(small, small_idx, std::max(1, R), std::max(1, M), seed, FTLM_START_PHILOX, bts,
-                                     n_bt, lnz_s, e_s);
+                                     n_bt, lnz_s, e_s, true);
   clear_and(FTLM_OK);
   if (rcf) return rcf;
+  if (lnz_s_err)  // the fused small sectors ran in complex128
+    for (int i : small_idx) std::fill(lnz_s_err + static_cast<size_t>(i) * n_bt, lnz_s_err + static_cast<size_t>(i + 1) * n_bt, 0.0);
   if (lnz_gc && n_avg && e_avg)
     return ftlm_gpu_gc_reduce(lnz_s, e_s, N.data(), nsec, bts, n_bt, mus, n_mu, n, lnz_gc, n_avg, e_avg);
   return FTLM_OK;
 }
+
+}  // namespace
 
 int ftlm_gpu_batched_release(void) {
   std::lock_guard<std::mutex> lock(g_bt_mu);

@@ -19,38 +19,64 @@ struct ChainGrad {
   double lmin = 0.0, g = 0.0, m[3] = {0.0, 0.0, 0.0};
 };
 
-// Weight matrices of up to nc chains, layout [i][ld][nc] (chain fastest), scales 1/(b_i b_l).
-int fill_weights(int nc, int ld, double bT, const std::vector<int>& n, const std::vector<double>& A,
-                 const std::vector<double>& B, const std::vector<std::vector<double>>& scale, std::vector<double>* Kp,
+// Weight matrices of up to nc chains on the GPU (symeig.cu: Jacobi eigen-decomposition of each
+// chain's tridiagonal, then K = Z P Z^T), written to g_grad.Kp in the layout [i][ld][nc] (chain
+// fastest) with the scales 1/(sc_i sc_l); g and the lowest Ritz value per chain to `out`.
+int fill_weights(ftlm_sector* s, int nc, int ld, double bT, const std::vector<int>& n, const std::vector<double>& A,
+                 const std::vector<double>& B, const std::vector<std::vector<double>>& scale,
                  std::vector<ChainGrad>* out) {
-  Kp->assign(static_cast<size_t>(ld) * ld * nc, 0.0);
-  std::vector<double> K;
+  cudaStream_t st = s->stream;
+  std::vector<double> sc(static_cast<size_t>(nc) * ld, 1.0);
+  for (int c = 0; c < nc; ++c)
+    for (size_t i = 0; i < scale[static_cast<size_t>(c)].size() && i < static_cast<size_t>(ld); ++i)
+      sc[static_cast<size_t>(c) * ld + i] = scale[static_cast<size_t>(c)][i];
+  const size_t mat = static_cast<size_t>(nc) * ld * sizeof(double);
+  DevBuf da, db, dn, dsc, dl, dvt, dy, dg, dlm, di;
+  CU_TRY(da.alloc(mat));
+  CU_TRY(db.alloc(mat));
+  CU_TRY(dn.alloc(nc * sizeof(int)));
+  CU_TRY(dsc.alloc(mat));
+  CU_TRY(dl.alloc(mat));
+  CU_TRY(dvt.alloc(mat * ld));
+  CU_TRY(dy.alloc(mat * ld));
+  CU_TRY(dg.alloc(nc * sizeof(double)));
+  CU_TRY(dlm.alloc(nc * sizeof(double)));
+  CU_TRY(di.alloc(nc * sizeof(int)));
+  CU_TRY(cudaMemcpyAsync(da.p, A.data(), mat, cudaMemcpyHostToDevice, st));
+  CU_TRY(cudaMemcpyAsync(db.p, B.data(), mat, cudaMemcpyHostToDevice, st));
+  CU_TRY(cudaMemcpyAsync(dn.p, n.data(), nc * sizeof(int), cudaMemcpyHostToDevice, st));
+  CU_TRY(cudaMemcpyAsync(dsc.p, sc.data(), mat, cudaMemcpyHostToDevice, st));
+  CU_TRY(cudaMemsetAsync(dg.p, 0, nc * sizeof(double), st));
+  CU_TRY(g_grad.grow(g_grad.Kp, g_grad.kcap, static_cast<size_t>(ld) * ld * nc * sizeof(double)));
+  CU_TRY(cudaMemsetAsync(g_grad.Kp.p, 0, static_cast<size_t>(ld) * ld * nc * sizeof(double), st));
+  CU_TRY(symeig_tridiag(da.as<double>(), db.as<double>(), dn.as<int>(), nc, ld, dl.as<double>(), nullptr,
+                        dvt.as<double>(), di.as<int>(), st));
+  CU_TRY(duhamel_weights_dev(dl.as<double>(), dvt.as<double>(), dn.as<int>(), nc, ld, bT, dsc.as<double>(),
+                             dy.as<double>(), g_grad.Kp.as<double>(), dg.as<double>(), dlm.as<double>(), st));
+  std::vector<double> g(static_cast<size_t>(nc)), lm(static_cast<size_t>(nc));
+  std::vector<int> info(static_cast<size_t>(nc));
+  CU_TRY(cudaMemcpyAsync(g.data(), dg.p, nc * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaMemcpyAsync(lm.data(), dlm.p, nc * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaMemcpyAsync(info.data(), di.p, nc * sizeof(int), cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaStreamSynchronize(st));
   for (int c = 0; c < nc; ++c) {
-    const int nn = n[static_cast<size_t>(c)];
     ChainGrad& cg = (*out)[static_cast<size_t>(c)];
     cg = ChainGrad{};
-    if (nn <= 0) continue;
-    K.assign(static_cast<size_t>(nn) * nn, 0.0);
-    const std::string err = duhamel_weights(nn, A.data() + static_cast<size_t>(c) * ld, B.data() + static_cast<size_t>(c) * ld,
-                                            bT, K.data(), &cg.g, &cg.lmin);
-    if (!err.empty()) return fail(FTLM_ERR_NUMERIC, err);
+    if (n[static_cast<size_t>(c)] <= 0) continue;
+    if (info[static_cast<size_t>(c)] != 0) return fail(FTLM_ERR_NUMERIC, "GPU Jacobi eigen-solver did not converge");
     cg.ok = true;
-    const std::vector<double>& sc = scale[static_cast<size_t>(c)];
-    for (int i = 0; i < nn; ++i)
-      for (int l = 0; l < nn; ++l)
-        (*Kp)[(static_cast<size_t>(i) * ld + l) * nc + c] =
-            K[static_cast<size_t>(i) * nn + l] / (sc[static_cast<size_t>(i)] * sc[static_cast<size_t>(l)]);
+    cg.g = g[static_cast<size_t>(c)];
+    cg.lmin = lm[static_cast<size_t>(c)];
   }
   return FTLM_OK;
 }
 
-// Moments of one batch of chains: Q [n][vstride], AQ likewise (or null), Kp [n][ld][nc].
+// Moments of one batch of chains: Q [n][vstride], AQ likewise (or null), weights already in
+// g_grad.Kp [n][ld][nc] (fill_weights).
 template <class T>
-int run_moments(ftlm_sector* s, const T* Q, const T* AQ, int64_t vstride, const std::vector<double>& Kp, int n, int ld,
-                int nc, std::vector<ChainGrad>* out) {
+int run_moments(ftlm_sector* s, const T* Q, const T* AQ, int64_t vstride, int n, int ld, int nc,
+                std::vector<ChainGrad>* out) {
   cudaStream_t st = s->stream;
-  CU_TRY(g_grad.grow(g_grad.Kp, g_grad.kcap, Kp.size() * sizeof(double)));
-  CU_TRY(cudaMemcpyAsync(g_grad.Kp.p, Kp.data(), Kp.size() * sizeof(double), cudaMemcpyHostToDevice, st));
   CU_TRY(g_grad.grow(g_grad.part, g_grad.pcap, static_cast<size_t>(2048) * 32 * 3 * sizeof(double)));
   int grid = 0;
   cudaError_t e;
@@ -102,11 +128,10 @@ int grad_plain(ftlm_sector* s, ftlm_sector* op, double bT, int R, int M, unsigne
         rc = op->apply(Q + static_cast<int64_t>(i) * dim, AQ + static_cast<int64_t>(i) * dim, s->stream);
         if (rc) return rc;
       }
-    std::vector<double> Kp;
     std::vector<std::vector<double>> scale(1, std::vector<double>(static_cast<size_t>(n), 1.0));
-    rc = fill_weights(1, M, bT, std::vector<int>{n}, A, B, scale, &Kp, &one);
+    rc = fill_weights(s, 1, M, bT, std::vector<int>{n}, A, B, scale, &one);
     if (rc) return rc;
-    rc = run_moments<double2>(s, Q, AQ, dim, Kp, n, M, 1, &one);
+    rc = run_moments<double2>(s, Q, AQ, dim, n, M, 1, &one);
     if (rc) return rc;
     (*out)[static_cast<size_t>(r)] = one[0];
   }
@@ -146,7 +171,7 @@ int grad_batched(ftlm_sector* s, ftlm_sector* op, double bT, int R, int M, unsig
     const unsigned seed_b = seed + static_cast<unsigned>(blk * kBtChains) * 100003u;
     CU_TRY(cudaMemsetAsync(al, 0, static_cast<size_t>(M) * kBtChains * sizeof(double), st));
     CU_TRY(cudaMemsetAsync(be, 0, static_cast<size_t>(M) * kBtChains * sizeof(double), st));
-    CU_TRY(bt_start(Q, dim, seed_b, sd, part, us, fl, st));
+    CU_TRY(bt_start(Q, dim, seed_b, sd, part, us, fl, st, &s->dev));
     CU_TRY(cudaMemcpyAsync(hs.data(), sd, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
     for (int k = 0; k < M; ++k)
       CU_TRY(bt_step(s->dev, Q + static_cast<int64_t>(k) * vs, Q + static_cast<int64_t>(k > 0 ? k - 1 : 0) * vs,
@@ -181,11 +206,10 @@ int grad_batched(ftlm_sector* s, ftlm_sector* op, double bT, int R, int M, unsig
       for (int i = 0; i < nmax; ++i)
         CU_TRY(bt_apply(op->dev, Q + static_cast<int64_t>(i) * vs, AQ + static_cast<int64_t>(i) * vs,
                         g_grad.stunit.as<double>(), part, g_grad.zflag.as<int>(), st));
-    std::vector<double> Kp;
     std::vector<ChainGrad> cg(static_cast<size_t>(kBtChains));
-    int rc = fill_weights(kBtChains, M, bT, n, A, B, scale, &Kp, &cg);
+    int rc = fill_weights(s, kBtChains, M, bT, n, A, B, scale, &cg);
     if (rc) return rc;
-    rc = run_moments<float2>(s, Q, AQ, vs, Kp, nmax, M, kBtChains, &cg);
+    rc = run_moments<float2>(s, Q, AQ, vs, nmax, M, kBtChains, &cg);
     if (rc) return rc;
     for (int c = 0; c < nc; ++c) (*out)[static_cast<size_t>(blk * kBtChains + c)] = cg[static_cast<size_t>(c)];
   }
@@ -209,6 +233,7 @@ int ftlm_gpu_grad_sector(ftlm_sector* s, ftlm_sector* op_tp, double bT, int R, i
   if (!lnz || !dlnz || method < 0 || method > 1) return fail(FTLM_ERR_INVALID, "bad arguments");
   R = std::max(1, R);
   M = std::max(1, M);
+  if (M > kMaxEig) return fail(FTLM_ERR_UNSUPPORTED, "more than 160 Lanczos steps for the GPU eigen-solver");
   const int64_t dim = s->plan.dim;
   std::vector<ChainGrad> cg;
   if (method == 1 && dim > 2 * static_cast<int64_t>(M)) {
@@ -420,42 +445,44 @@ int ftlm_gpu_gc_logz_grad(const ftlm_params* p, double mu, double bT, int R, int
   return FTLM_OK;
 }
 
-// Per-chain log quadrature and energy ratio with a converged eigen-decomposition (host QL), the
-// quadrature the gradient differentiates; same layout as ftlm_gpu_tridiag_quadrature.
+// Per-chain log quadrature and energy ratio with a converged eigen-decomposition (parallel cyclic
+// Jacobi on the GPU, symeig.cu), the quadrature the gradient differentiates; same layout as
+// ftlm_gpu_tridiag_quadrature.
 int ftlm_gpu_tridiag_quadrature_exact(const double* alpha, const double* beta, const int* n, int nc, int ld,
                                       const double* bts, int n_bt, double* logq, double* energy) {
   if (nc < 0 || ld <= 0 || n_bt < 0 || !alpha || !beta || !n || (n_bt > 0 && (!bts || !logq || !energy)))
     return fail(FTLM_ERR_INVALID, "bad arguments");
-  std::vector<double> lam, Z;
-  for (int c = 0; c < nc; ++c) {
-    const int nn = n[c];
-    if (nn > ld) return fail(FTLM_ERR_INVALID, "chain length exceeds ld");
-    double* lq = logq + static_cast<size_t>(c) * n_bt;
-    double* eq = energy + static_cast<size_t>(c) * n_bt;
-    if (nn <= 0) {
-      for (int b = 0; b < n_bt; ++b) {
-        lq[b] = -std::numeric_limits<double>::infinity();
-        eq[b] = 0.0;
-      }
-      continue;
-    }
-    lam.assign(static_cast<size_t>(nn), 0.0);
-    Z.assign(static_cast<size_t>(nn) * nn, 0.0);
-    const std::string err = tridiag_eigvec(nn, alpha + static_cast<size_t>(c) * ld, beta + static_cast<size_t>(c) * ld,
-                                           lam.data(), Z.data());
-    if (!err.empty()) return fail(FTLM_ERR_NUMERIC, err);
-    for (int b = 0; b < n_bt; ++b) {
-      const double bT = bts[b];
-      double z = 0.0, ze = 0.0;
-      for (int j = 0; j < nn; ++j) {
-        const double w = Z[static_cast<size_t>(j)] * Z[static_cast<size_t>(j)] * std::exp(-bT * (lam[static_cast<size_t>(j)] - lam[0]));
-        z += w;
-        ze += w * lam[static_cast<size_t>(j)];
-      }
-      lq[b] = -bT * lam[0] + std::log(z);
-      eq[b] = ze / z;
-    }
-  }
+  if (ld > kMaxEig) return fail(FTLM_ERR_UNSUPPORTED, "tridiagonal size > 160 is not supported by the GPU eigen-solver");
+  for (int c = 0; c < nc; ++c)
+    if (n[c] < 0 || n[c] > ld) return fail(FTLM_ERR_INVALID, "chain length outside [0, ld]");
+  if (static_cast<long long>(nc) * n_bt > 0x7fffffffLL) return fail(FTLM_ERR_INVALID, "n_chains * n_bt exceeds 2^31 - 1");
+  if (nc == 0 || n_bt == 0) return FTLM_OK;
+  const size_t mat = static_cast<size_t>(nc) * ld * sizeof(double);
+  const size_t outb = static_cast<size_t>(nc) * n_bt * sizeof(double);
+  DevBuf da, db, dn, dl, dw, dbt, dq, de, di;
+  CU_TRY(da.alloc(mat));
+  CU_TRY(db.alloc(mat));
+  CU_TRY(dn.alloc(nc * sizeof(int)));
+  CU_TRY(dl.alloc(mat));
+  CU_TRY(dw.alloc(mat));
+  CU_TRY(dbt.alloc(n_bt * sizeof(double)));
+  CU_TRY(dq.alloc(outb));
+  CU_TRY(de.alloc(outb));
+  CU_TRY(di.alloc(nc * sizeof(int)));
+  CU_TRY(cudaMemcpy(da.p, alpha, mat, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(db.p, beta, mat, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(dn.p, n, nc * sizeof(int), cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(dbt.p, bts, n_bt * sizeof(double), cudaMemcpyHostToDevice));
+  CU_TRY(symeig_tridiag(da.as<double>(), db.as<double>(), dn.as<int>(), nc, ld, dl.as<double>(), dw.as<double>(),
+                        nullptr, di.as<int>(), nullptr));
+  CU_TRY(quad_eval(dl.as<double>(), dw.as<double>(), dn.as<int>(), nc, ld, dbt.as<double>(), n_bt, dq.as<double>(),
+                   de.as<double>(), nullptr));
+  std::vector<int> info(static_cast<size_t>(nc));
+  CU_TRY(cudaMemcpy(info.data(), di.p, nc * sizeof(int), cudaMemcpyDeviceToHost));
+  for (int c = 0; c < nc; ++c)
+    if (n[c] > 0 && info[static_cast<size_t>(c)] != 0) return fail(FTLM_ERR_NUMERIC, "GPU Jacobi eigen-solver did not converge");
+  CU_TRY(cudaMemcpy(logq, dq.p, outb, cudaMemcpyDeviceToHost));
+  CU_TRY(cudaMemcpy(energy, de.p, outb, cudaMemcpyDeviceToHost));
   return FTLM_OK;
 }
 

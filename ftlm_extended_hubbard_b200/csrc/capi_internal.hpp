@@ -21,6 +21,7 @@
 #include "hv.cuh"
 #include "orbit.cuh"
 #include "plan.hpp"
+#include "symeig.cuh"
 #include "tridiag.hpp"
 
 namespace ftlm_b200 {
@@ -77,6 +78,13 @@ void reference_start(int64_t dim, unsigned seed, std::vector<std::complex<double
 struct LanczosWs {
   int64_t n = 0;
   DevBuf q, qp, w, scratch;
+  DevBuf dotp;  // column-pass partials of the fused sector recurrence
+  int64_t dotp_n = 0;
+  cudaError_t ensure_dotp(int64_t nblocks) {
+    if (nblocks <= dotp_n && dotp.p) return cudaSuccess;
+    dotp_n = nblocks;
+    return dotp.alloc(static_cast<size_t>(nblocks) * 2 * sizeof(double));
+  }
   cudaError_t ensure(int64_t dim) {
     if (n == dim && q.p) return cudaSuccess;
     n = dim;
@@ -152,7 +160,7 @@ struct ftlm_sector {
   int device = -1;
   ftlm_b200::DevSector dev{};
   std::vector<void*> owned;
-  int apply_path = 0;    // 0 auto, 1 generic, 2 rows+cols
+  int apply_path = 0;    // 0 auto, 1 generic, 2 rows+cols, 3 rows (register coefficient classes)+cols
   int cols_variant = 0;  // column-slab width of path 2 (hv_launch)
   ftlm_b200::capi::LanczosWs ws;
   ftlm_b200::capi::DevBuf hx, hy;  // staging for the host-buffer apply
@@ -162,14 +170,23 @@ struct ftlm_sector {
     if (stream) cudaStreamDestroy(stream);
   }
   int effective_path() const {
-    if (apply_path == 1 || apply_path == 2) return apply_path;
-    return ftlm_b200::hv_fast_path_ok(dev, plan.max_up_deg) ? 2 : 1;
+    if (apply_path >= 1 && apply_path <= 3) return (apply_path == 3 && !dev.dn_ent4) ? 2 : apply_path;
+    return ftlm_b200::hv_fast_path_ok(dev_for(2), plan.max_up_deg) ? 2 : 1;
+  }
+  // The device view a launch of `path` uses: the row pass takes its coefficients from the per-row
+  // shared-memory table (path 2), or from register-held coefficient classes with the compact entry
+  // table (path 3, where the sector has one).
+  ftlm_b200::DevSector dev_for(int path) const {
+    ftlm_b200::DevSector d = dev;
+    if (path != 3) d.dn_ent4 = nullptr;
+    return d;
   }
   int apply(const double2* x, double2* y, cudaStream_t st) {
     const int path = effective_path();
-    if (path == 2 && ftlm_b200::hv_rows_smem_bytes(dev) > 227 * 1024)
+    const ftlm_b200::DevSector d = dev_for(path);
+    if (path >= 2 && ftlm_b200::hv_rows_smem_bytes(d) > 227 * 1024)
       return ftlm_b200::capi::fail(FTLM_ERR_UNSUPPORTED, "row pass does not fit in shared memory for this sector");
-    CU_TRY(ftlm_b200::hv_launch(dev, x, y, path, st, cols_variant));
+    CU_TRY(ftlm_b200::hv_launch(d, x, y, path == 3 ? 2 : path, st, cols_variant));
     return FTLM_OK;
   }
 };
@@ -235,7 +252,7 @@ extern GradWs g_grad;
 // Runs ceil(R/32) blocks of 32 chains on sector s; A/B [R][M] (beta zero-padded), used [R].
 template <class Step>
 int bt_run_chains_impl(int64_t dim, cudaStream_t st, Step&& step, int R, int M, unsigned seed, std::vector<double>* A,
-                       std::vector<double>* B, std::vector<int>* used) {
+                       std::vector<double>* B, std::vector<int>* used, const DevSector* gauge) {
   A->assign(static_cast<size_t>(R) * M, 0.0);
   B->assign(static_cast<size_t>(R) * M, 0.0);
   used->assign(static_cast<size_t>(R), 0);
@@ -254,7 +271,7 @@ int bt_run_chains_impl(int64_t dim, cudaStream_t st, Step&& step, int R, int M, 
     const unsigned seed_b = seed + static_cast<unsigned>(blk * kBtChains) * 100003u;
     CU_TRY(cudaMemsetAsync(al, 0, static_cast<size_t>(M) * kBtChains * sizeof(double), st));
     CU_TRY(cudaMemsetAsync(be, 0, static_cast<size_t>(M) * kBtChains * sizeof(double), st));
-    CU_TRY(bt_start(bufs[0], dim, seed_b, sd, part, us, fl, st));
+    CU_TRY(bt_start(bufs[0], dim, seed_b, sd, part, us, fl, st, gauge));
     cudaGraph_t graph = nullptr;
     CU_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     float2 *wk = bufs[0], *y = bufs[1], *wkm1 = bufs[2];
@@ -297,10 +314,21 @@ int bt_run_chains_impl(int64_t dim, cudaStream_t st, Step&& step, int R, int M, 
   return FTLM_OK;
 }
 
+// Per-chain log quadrature and energy (layout of ftlm_gpu_tridiag_quadrature) with the reference's
+// rotation-capped Jacobi (converged == false) or the converged GPU eigen-decomposition.
+int chain_quadrature(const double* A, const double* B, const int* n, int nc, int ld, const double* bts, int n_bt,
+                     double* lq, double* eq, bool converged);
+// The quadrature of the complex128 sector path (ftlm_gpu_set_quadrature; the reference's Jacobi by default).
+bool plain_quadrature_converged();
+// ftlm_gpu_ftlm_sector with an explicit quadrature choice.
+int plain_sector_ftlm(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed, int start_mode,
+                      bool converged, double* lnz, double* energy);
+
 // ftlm_gpu_ftlm_sector for many small sectors in one chains_lanczos launch (capi.cu); results in
 // rows out_idx[i] of lnz_s / e_s.
 int fused_sectors_ftlm(const std::vector<ftlm_sector*>& secs, const std::vector<int>& out_idx, int R, int M,
-                       unsigned seed, int start_mode, const double* bts, int n_bt, double* lnz_s, double* e_s);
+                       unsigned seed, int start_mode, const double* bts, int n_bt, double* lnz_s, double* e_s,
+                       bool converged);
 
 // 32-chain blocks of one sector (bt_step), alpha/beta [R][M], steps used [R].
 int bt_run_chains(ftlm_sector* s, int R, int M, unsigned seed, std::vector<double>* A, std::vector<double>* B,

@@ -374,7 +374,8 @@ int ftlm_gpu_orbit_ftlm(ftlm_orbit* o, const double* bts, int n_bt, int R, int M
     nv[static_cast<size_t>(r)] = static_cast<int>(a.size());
   }
   std::vector<double> lq(static_cast<size_t>(R) * n_bt), eq(static_cast<size_t>(R) * n_bt);
-  int rc = ftlm_gpu_tridiag_quadrature(A.data(), B.data(), nv.data(), R, M, bts, n_bt, lq.data(), eq.data());
+  int rc = chain_quadrature(A.data(), B.data(), nv.data(), R, M, bts, n_bt, lq.data(), eq.data(),
+                            plain_quadrature_converged());
   if (rc) return rc;
   return ftlm_gpu_ftlm_combine(lq.data(), eq.data(), nv.data(), R, n_bt, std::log(static_cast<double>(dk)), lnz, energy);
 }
@@ -401,23 +402,35 @@ int ftlm_gpu_orbit_batched_ftlm(ftlm_orbit* o, const double* bts, int n_bt, int 
       dk, st,
       [&Adev, st](const float2* wk, const float2* wkm1, float2* y, int k, double* sd, double* part, double* al,
                   double* be, int* us, int* fl) { return bt_orbit_step(Adev, wk, wkm1, y, k, sd, part, al, be, us, fl, st); },
-      R, M, seed, &A, &B, &used);
+      R, M, seed, &A, &B, &used, nullptr);
   if (rc) return rc;
   std::vector<double> lq(static_cast<size_t>(R) * n_bt), eq(static_cast<size_t>(R) * n_bt);
-  rc = ftlm_gpu_tridiag_quadrature(A.data(), B.data(), used.data(), R, M, bts, n_bt, lq.data(), eq.data());
+  rc = chain_quadrature(A.data(), B.data(), used.data(), R, M, bts, n_bt, lq.data(), eq.data(), true);
   if (rc) return rc;
   return ftlm_gpu_ftlm_combine(lq.data(), eq.data(), used.data(), R, n_bt, std::log(static_cast<double>(dk)), lnz, energy);
 }
 
 // Exact ln Tr e^{-bT H_K} of a small block (the k-bench's exact_log_partition_small_complex,
-// benchmarks/bench_ftlm_nmu_4x4_k.cpp:249-333): H_K built on the GPU column by column, eigenvalues of
-// its real 2dk x 2dk embedding [[Re, -Im], [Im, Re]] (each eigenvalue twice) on the host.
+// benchmarks/bench_ftlm_nmu_4x4_k.cpp:249-333), all on the GPU: H_K built column by column, its
+// real 2dk x 2dk embedding [[Re, -Im], [Im, Re]] (each eigenvalue twice) diagonalised by the
+// parallel Jacobi of symeig.cu, and ln Z = log sum_i (1/2) e^{-bT lam_i} with the energy ratio by
+// the quadrature evaluation kernel (weights 1/2).  2dk <= 160.
 static int orbit_block_ed(ftlm_orbit* o, const double* bts, int n_bt, double* lnz, double* energy) {
   const int64_t dk = o->dk;
+  const int m = static_cast<int>(2 * dk);
+  if (m > kMaxEig) return fail(FTLM_ERR_UNSUPPORTED, "exact small-block path: block dimension > 80");
   const size_t col = static_cast<size_t>(dk) * sizeof(double2);
-  DevBuf X, Y;
+  DevBuf X, Y, Rm, lam, w, nn, bt, lq, eq, info;
   CU_TRY(X.alloc(col * dk));
   CU_TRY(Y.alloc(col * dk));
+  CU_TRY(Rm.alloc(static_cast<size_t>(m) * m * sizeof(double)));
+  CU_TRY(lam.alloc(static_cast<size_t>(m) * sizeof(double)));
+  CU_TRY(w.alloc(static_cast<size_t>(m) * sizeof(double)));
+  CU_TRY(nn.alloc(sizeof(int)));
+  CU_TRY(bt.alloc(std::max(1, n_bt) * sizeof(double)));
+  CU_TRY(lq.alloc(std::max(1, n_bt) * sizeof(double)));
+  CU_TRY(eq.alloc(std::max(1, n_bt) * sizeof(double)));
+  CU_TRY(info.alloc(sizeof(int)));
   cudaStream_t st = o->sector->stream;
   CU_TRY(cudaMemsetAsync(X.p, 0, col * dk, st));
   const double one[2] = {1.0, 0.0};
@@ -427,31 +440,22 @@ static int orbit_block_ed(ftlm_orbit* o, const double* bts, int n_bt, double* ln
     const int rc = orbit_apply_dev(o, X.as<double2>() + j * dk, Y.as<double2>() + j * dk, st);
     if (rc) return rc;
   }
-  std::vector<double> H(static_cast<size_t>(dk) * dk * 2);  // column j = H_K e_j
-  CU_TRY(cudaMemcpyAsync(H.data(), Y.p, col * dk, cudaMemcpyDeviceToHost, st));
-  CU_TRY(cudaStreamSynchronize(st));
-  const int m = static_cast<int>(2 * dk);
-  std::vector<double> Rm(static_cast<size_t>(m) * m), lam(static_cast<size_t>(m));
-  for (int64_t j = 0; j < dk; ++j)
-    for (int64_t i = 0; i < dk; ++i) {
-      const double re = H[2 * (static_cast<size_t>(j) * dk + i)], im = H[2 * (static_cast<size_t>(j) * dk + i) + 1];
-      Rm[static_cast<size_t>(i) * m + j] = re;
-      Rm[static_cast<size_t>(i) * m + j + dk] = -im;
-      Rm[static_cast<size_t>(i + dk) * m + j] = im;
-      Rm[static_cast<size_t>(i + dk) * m + j + dk] = re;
-    }
-  const std::string err = sym_eigvals(m, Rm.data(), lam.data());
-  if (!err.empty()) return fail(FTLM_ERR_NUMERIC, err);
-  for (int b = 0; b < n_bt; ++b) {
-    double z = 0.0, ze = 0.0;
-    for (int i = 0; i < m; ++i) {
-      const double w = std::exp(-bts[b] * (lam[static_cast<size_t>(i)] - lam[0]));
-      z += w;
-      ze += w * lam[static_cast<size_t>(i)];
-    }
-    lnz[b] = std::log(0.5) - bts[b] * lam[0] + std::log(z);
-    energy[b] = ze / z;
+  const std::vector<double> half(static_cast<size_t>(m), 0.5);
+  CU_TRY(cudaMemcpyAsync(w.p, half.data(), m * sizeof(double), cudaMemcpyHostToDevice, st));
+  CU_TRY(cudaMemcpyAsync(nn.p, &m, sizeof(int), cudaMemcpyHostToDevice, st));
+  if (n_bt > 0) CU_TRY(cudaMemcpyAsync(bt.p, bts, n_bt * sizeof(double), cudaMemcpyHostToDevice, st));
+  CU_TRY(embed_hermitian(Y.as<double2>(), static_cast<int>(dk), Rm.as<double>(), st));
+  CU_TRY(symeig_dense(Rm.as<double>(), nn.as<int>(), 1, m, lam.as<double>(), info.as<int>(), st));
+  CU_TRY(quad_eval(lam.as<double>(), w.as<double>(), nn.as<int>(), 1, m, bt.as<double>(), n_bt, lq.as<double>(),
+                   eq.as<double>(), st));
+  int h_info = 0;
+  CU_TRY(cudaMemcpyAsync(&h_info, info.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  if (n_bt > 0) {
+    CU_TRY(cudaMemcpyAsync(lnz, lq.p, n_bt * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CU_TRY(cudaMemcpyAsync(energy, eq.p, n_bt * sizeof(double), cudaMemcpyDeviceToHost, st));
   }
+  CU_TRY(cudaStreamSynchronize(st));
+  if (h_info != 0) return fail(FTLM_ERR_NUMERIC, "GPU Jacobi eigen-solver did not converge");
   return FTLM_OK;
 }
 

@@ -25,10 +25,16 @@ struct DevSector {
   const uint32_t* dn_csr_ent;
   const float2* up_coef32;     // [nnz_up] complex64 copies for the batched path
   const float2* dn_coef32;     // [n_dn_hops+1]
+  const float2* dn_coef32s;    // [2*(n_dn_hops+1)]: [2*hop + s] = (-1)^s coef (the gauge-basis row pass)
   const double2* dn_coef;  // [n_dn_hops+1]
   const uint32_t* dn_nmask;// [n_dn_hops+1]
   int n_dn_hops;           // == pad hop id
   int* flags;              // [0]: input has a non-zero entry with |x|^2 < 1e-28
+  // Compact row-pass table (plan.hpp, SectorPlan::dn_compact); dn_ent4 == nullptr when absent.
+  const uint4* dn_ent4;    // [group][round/4][lane] x 4 entries
+  const int64_t* dn_gptr4; // [ngroups+1], offsets in entries
+  double dn_re[4], dn_im[4];
+  int dn_re_bits, dn_im_bits;  // class-index widths; dn_im_bits < 0: all coefficients real
 };
 
 // The reference skips source columns with std::norm(x) < 1e-28
@@ -49,6 +55,14 @@ __device__ __forceinline__ uint32_t prefix_parity_shifted(uint32_t d) {
 __device__ __forceinline__ double diag_value(const DevSector& S, uint32_t u, uint32_t d, int cuu, int cdd, uint4 w) {
   const int cross = __popc(d & w.x) + 2 * __popc(d & w.y) + 4 * __popc(d & w.z) + 8 * __popc(d & w.w);
   return S.U * static_cast<double>(__popc(u & d)) + S.V * static_cast<double>(cuu + cdd + cross);
+}
+
+// Sign of the basis state (u, d) in the spin-ordered ("gauge") basis: with
+// g = (-1)^{#(up site, down site) pairs with the down site below the up site}, G H G (G = diag g)
+// is diag + U x 1 + 1 x D, the up-hop part independent of the down string and the down-hop part
+// independent of the up string (each keeps only its own species' Jordan-Wigner signs).
+__device__ __forceinline__ uint32_t gauge_sign(uint32_t u, uint32_t d) {
+  return static_cast<uint32_t>(__popc(u & prefix_parity_shifted(d))) & 1u;
 }
 
 // acc += (neg ? -c : c) * v   (complex)

@@ -8,6 +8,9 @@
 //   hv_rows     pass 1 of the fast path: persistent CTAs, one output row at a time; the input
 //               row is staged in shared memory (down hops gather inside it); writes
 //               y = diag o x + down part.  Requires a down row (+ coefficient table) to fit in SMEM.
+//               Two forms: hv_rows_compact (coefficient classes in registers, compact 4-entry
+//               loads; the default where the sector's down hops allow it) and hv_rows (per-row
+//               coefficient table in shared memory; any hop list).
 //   hv_cols     pass 2: CTA = (output row, 256-column chunk, two columns per thread), chunk-major so that
 //               the 256-column slab of x stays resident in L2 while all rows read it; adds the
 //               up part: y[r, c] += sum_j coef_j * s_j(c) * x[src_j, c].
@@ -31,7 +34,7 @@ __global__ void __launch_bounds__(256) hv_generic_kernel(DevSector S, const doub
 constexpr int kRowThreads = 1024;
 
 __global__ void __launch_bounds__(kRowThreads, 1) hv_rows_kernel(DevSector S, const double2* __restrict__ x,
-                                                                   double2* __restrict__ y) {
+                                                                   double2* __restrict__ y, double sx) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int Dd = static_cast<int>(S.Dd);
   double2* xs = reinterpret_cast<double2*>(smem_raw);
@@ -54,6 +57,8 @@ __global__ void __launch_bounds__(kRowThreads, 1) hv_rows_kernel(DevSector S, co
     int saw_tiny = 0;
     for (int c = tid; c < Dd; c += kRowThreads) {
       double2 v = xrow[c];
+      v.x *= sx;  // the input is sx * x (sx = 1: unchanged)
+      v.y *= sx;
       if (tiny(v)) {
         saw_tiny |= (v.x != 0.0 || v.y != 0.0);
         v = make_double2(0.0, 0.0);
@@ -91,6 +96,128 @@ __global__ void __launch_bounds__(kRowThreads, 1) hv_rows_kernel(DevSector S, co
   }
 }
 
+// Row pass with the compact down-hop table (SectorPlan::dn_compact): the hop's coefficient comes
+// from a 4-entry class table held in registers (real part, |imaginary part|, sign bit) and its
+// per-row up-string factor from the prefix parity of u, so each hop costs one 16-byte shared load
+// (the x gather) and no coefficient-table load; entries arrive 4 at a time (16-byte loads, two
+// loads ahead).  Same terms in the same order as hv_rows_kernel (the same sums).
+template <int KB>
+__device__ __forceinline__ double pick_class(uint32_t k, const double (&t)[4]) {
+  if constexpr (KB <= 0) {
+    return t[0];
+  } else if constexpr (KB == 1) {
+    return (k & 1u) ? t[1] : t[0];
+  } else {
+    return (k & 2u) ? ((k & 1u) ? t[3] : t[2]) : ((k & 1u) ? t[1] : t[0]);
+  }
+}
+
+__device__ __forceinline__ double flip_sign(double v, uint32_t neg) {
+  return __hiloint2double(__double2hiint(v) ^ static_cast<int>(neg << 31), __double2loint(v));
+}
+
+template <int KR, int KI>
+__device__ __forceinline__ void row_term(double2& acc, uint32_t e, const double2* xs, uint32_t qu,
+                                         const double (&re)[4], const double (&im)[4]) {
+  const double2 v = xs[e & 0x3FFFu];
+  const uint32_t neg = ((qu >> ((e >> 14) & 31u)) ^ (qu >> ((e >> 19) & 31u)) ^ (e >> 24)) & 1u;
+  const double cr = flip_sign(pick_class<KR>((e >> 25) & 3u, re), neg);
+  acc.x = fma(cr, v.x, acc.x);
+  if constexpr (KI >= 0) {
+    const double ci = flip_sign(pick_class<KI>((e >> 27) & 3u, im), neg ^ ((e >> 29) & 1u));
+    acc.x = fma(-ci, v.y, acc.x);
+    acc.y = fma(cr, v.y, acc.y);
+    acc.y = fma(ci, v.x, acc.y);
+  } else {
+    acc.y = fma(cr, v.y, acc.y);
+  }
+}
+
+template <int KR, int KI>
+__global__ void __launch_bounds__(kRowThreads, 1) hv_rows_compact_kernel(DevSector S, const double2* __restrict__ x,
+                                                                           double2* __restrict__ y, double sx) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int Dd = static_cast<int>(S.Dd);
+  double2* xs = reinterpret_cast<double2*>(smem_raw);
+  const int tid = threadIdx.x;
+  double re[4], im[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    re[i] = S.dn_re[i];
+    im[i] = S.dn_im[i];
+  }
+  if (tid < 8) xs[Dd + tid] = make_double2(0.0, 0.0);  // zero sentinels for padding entries
+  for (int64_t r = blockIdx.x; r < S.Du; r += gridDim.x) {
+    if (tid == 0 && r + gridDim.x < S.Du) {
+      const char* nxt = reinterpret_cast<const char*>(x + (r + gridDim.x) * S.Dd);
+      const uint32_t bytes = static_cast<uint32_t>(S.Dd * sizeof(double2));
+      for (uint32_t off = 0; off < bytes; off += 32768u) {
+        const uint32_t sz = min(32768u, bytes - off);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(nxt + off), "r"(sz) : "memory");
+      }
+    }
+    const uint32_t u = S.umask[r];
+    const uint32_t qu = prefix_parity_shifted(u);
+    const int cuu = S.cnt_uu[r];
+    const uint4 w = S.wpl[r];
+    const double2* xrow = x + r * S.Dd;
+    int saw_tiny = 0;
+    for (int c = tid; c < Dd; c += kRowThreads) {
+      double2 v = xrow[c];
+      v.x *= sx;
+      v.y *= sx;
+      if (tiny(v)) {
+        saw_tiny |= (v.x != 0.0 || v.y != 0.0);
+        v = make_double2(0.0, 0.0);
+      }
+      xs[c] = v;
+    }
+    if (saw_tiny) atomicOr(S.flags, 1);
+    __syncthreads();
+    double2* yrow = y + r * S.Dd;
+    for (int c = tid; c < Dd; c += kRowThreads) {
+      const double2 xv = xs[c];
+      const double dg = diag_value(S, u, S.dmask[c], cuu, S.cnt_dd[c], w);
+      double2 acc = make_double2(dg * xv.x, dg * xv.y);
+      const int g = c >> 5;
+      const int64_t b0 = S.dn_gptr4[g];
+      const int nq = static_cast<int>((S.dn_gptr4[g + 1] - b0) >> 7);  // 16-byte loads per lane
+      const uint4* ep = S.dn_ent4 + (b0 >> 2) + (c & 31);
+      uint4 cur = __ldg(ep);
+      uint4 nxt = nq > 1 ? __ldg(ep + 32) : cur;
+      for (int q = 0; q < nq; ++q) {
+        const uint4 e = cur;
+        cur = nxt;
+        if (q + 2 < nq) nxt = __ldg(ep + (q + 2) * 32);
+        row_term<KR, KI>(acc, e.x, xs, qu, re, im);
+        row_term<KR, KI>(acc, e.y, xs, qu, re, im);
+        row_term<KR, KI>(acc, e.z, xs, qu, re, im);
+        row_term<KR, KI>(acc, e.w, xs, qu, re, im);
+      }
+      yrow[c] = acc;
+    }
+    __syncthreads();
+  }
+}
+
+using RowsKernel = void (*)(DevSector, const double2*, double2*, double);
+
+template <int KR>
+RowsKernel rows_compact_for(int ki) {
+  switch (ki) {
+    case -1: return hv_rows_compact_kernel<KR, -1>;
+    case 0: return hv_rows_compact_kernel<KR, 0>;
+    case 1: return hv_rows_compact_kernel<KR, 1>;
+    default: return hv_rows_compact_kernel<KR, 2>;
+  }
+}
+
+RowsKernel rows_compact(int kr, int ki) {
+  if (kr <= 0) return rows_compact_for<0>(ki);
+  if (kr == 1) return rows_compact_for<1>(ki);
+  return rows_compact_for<2>(ki);
+}
+
 // Column pass: two columns per thread, chunk = 2 * threads columns (variants: 64 / 128 / 256
 // threads = 128 / 256 / 512-column slabs of Du * chunk * 16 bytes kept in L2; the autotuner picks).
 constexpr int kMaxUpDeg = 128;
@@ -106,20 +233,24 @@ __device__ __forceinline__ void cmac_xor(double2& acc, double2 c, double2 v, uin
   acc.y = fma(c.y, v.x, acc.y);
 }
 
-template <int kColThreads, bool kFilter>
+// kFused: the input is sx * x; the up-hop sum is formed on its own and added as
+// y = y_rows + sx * sum, and the thread's share of <sx x, y> over its columns goes to dot
+// (the Lanczos step's alpha without a separate pass: x[r, c] is in the L2-resident slab).
+template <int kColThreads, bool kFilter, bool kFused>
 __device__ __forceinline__ void cols_body(const DevSector& S, const double2* __restrict__ x, double2* __restrict__ y,
                                           int64_t r, int64_t c0, int deg, const int64_t* s_off, const double2* s_coef,
-                                          const uint32_t* s_lh) {
+                                          const uint32_t* s_lh, double sx, double (&dot)[2]) {
   const int64_t c1 = c0 + kColThreads;
   const bool has1 = c1 < S.Dd;
   const int64_t c1s = has1 ? c1 : c0;  // in-bounds column for the second lane slot
   const uint32_t q0 = prefix_parity_shifted(S.dmask[c0]);
   const uint32_t q1 = prefix_parity_shifted(S.dmask[c1s]);
   double2* y0 = y + r * S.Dd + c0;
-  double2 acc0 = *y0;
-  double2 acc1 = has1 ? y[r * S.Dd + c1] : make_double2(0.0, 0.0);
+  double2 acc0 = kFused ? make_double2(0.0, 0.0) : *y0;
+  double2 acc1 = (has1 && !kFused) ? y[r * S.Dd + c1] : make_double2(0.0, 0.0);
   const double2* x0 = x + c0;
   const double2* x1 = x + c1s;
+  auto skip = [sx](double2 v) { return kFused ? tiny(make_double2(sx * v.x, sx * v.y)) : tiny(v); };
   int j = 0;
   for (; j + 4 <= deg; j += 4) {
     double2 v0[4], v1[4];
@@ -134,8 +265,8 @@ __device__ __forceinline__ void cols_body(const DevSector& S, const double2* __r
       const uint32_t lh = s_lh[j + t];
       const uint32_t lo = lh & 255u, hi = lh >> 8;
       const double2 cf = s_coef[j + t];
-      if (!kFilter || !tiny(v0[t])) cmac_xor(acc0, cf, v0[t], ((q0 >> lo) ^ (q0 >> hi)) & 1u);
-      if (!kFilter || !tiny(v1[t])) cmac_xor(acc1, cf, v1[t], ((q1 >> lo) ^ (q1 >> hi)) & 1u);
+      if (!kFilter || !skip(v0[t])) cmac_xor(acc0, cf, v0[t], ((q0 >> lo) ^ (q0 >> hi)) & 1u);
+      if (!kFilter || !skip(v1[t])) cmac_xor(acc1, cf, v1[t], ((q1 >> lo) ^ (q1 >> hi)) & 1u);
     }
   }
   for (; j < deg; ++j) {
@@ -144,16 +275,33 @@ __device__ __forceinline__ void cols_body(const DevSector& S, const double2* __r
     const uint32_t lh = s_lh[j];
     const uint32_t lo = lh & 255u, hi = lh >> 8;
     const double2 cf = s_coef[j];
-    if (!kFilter || !tiny(v0)) cmac_xor(acc0, cf, v0, ((q0 >> lo) ^ (q0 >> hi)) & 1u);
-    if (!kFilter || !tiny(v1)) cmac_xor(acc1, cf, v1, ((q1 >> lo) ^ (q1 >> hi)) & 1u);
+    if (!kFilter || !skip(v0)) cmac_xor(acc0, cf, v0, ((q0 >> lo) ^ (q0 >> hi)) & 1u);
+    if (!kFilter || !skip(v1)) cmac_xor(acc1, cf, v1, ((q1 >> lo) ^ (q1 >> hi)) & 1u);
+  }
+  if constexpr (kFused) {
+    const double2 r0 = *y0;
+    acc0 = make_double2(fma(sx, acc0.x, r0.x), fma(sx, acc0.y, r0.y));
+    const double2 xq0 = x[r * S.Dd + c0];
+    const double qx = sx * xq0.x, qy = sx * xq0.y;  // conj(q) * y
+    dot[0] += qx * acc0.x + qy * acc0.y;
+    dot[1] += qx * acc0.y - qy * acc0.x;
+    if (has1) {
+      const double2 r1 = y[r * S.Dd + c1];
+      acc1 = make_double2(fma(sx, acc1.x, r1.x), fma(sx, acc1.y, r1.y));
+      const double2 xq1 = x[r * S.Dd + c1];
+      const double px = sx * xq1.x, py = sx * xq1.y;
+      dot[0] += px * acc1.x + py * acc1.y;
+      dot[1] += px * acc1.y - py * acc1.x;
+    }
   }
   *y0 = acc0;
   if (has1) y[r * S.Dd + c1] = acc1;
 }
 
-template <int kColThreads>
+template <int kColThreads, bool kFused>
 __global__ void __launch_bounds__(kColThreads) hv_cols_kernel(DevSector S, const double2* __restrict__ x,
-                                                              double2* __restrict__ y) {
+                                                              double2* __restrict__ y, double sx,
+                                                              double* __restrict__ dotp) {
   constexpr int kColChunk = 2 * kColThreads;
   __shared__ int64_t s_off[kMaxUpDeg];
   __shared__ double2 s_coef[kMaxUpDeg];
@@ -171,11 +319,30 @@ __global__ void __launch_bounds__(kColThreads) hv_cols_kernel(DevSector S, const
   const bool filt = (*S.flags) != 0;
   __syncthreads();
   const int64_t c0 = chunk * kColChunk + threadIdx.x;
-  if (c0 >= S.Dd) return;
-  if (filt)
-    cols_body<kColThreads, true>(S, x, y, r, c0, deg, s_off, s_coef, s_lh);
-  else
-    cols_body<kColThreads, false>(S, x, y, r, c0, deg, s_off, s_coef, s_lh);
+  double dot[2] = {0.0, 0.0};
+  if (c0 < S.Dd) {
+    if (filt)
+      cols_body<kColThreads, true, kFused>(S, x, y, r, c0, deg, s_off, s_coef, s_lh, sx, dot);
+    else
+      cols_body<kColThreads, false, kFused>(S, x, y, r, c0, deg, s_off, s_coef, s_lh, sx, dot);
+  }
+  if constexpr (kFused) {  // fixed tree over the block: one (re, im) partial per block
+    __shared__ double red[2][kColThreads];
+    red[0][threadIdx.x] = dot[0];
+    red[1][threadIdx.x] = dot[1];
+    __syncthreads();
+    for (int h = kColThreads / 2; h > 0; h >>= 1) {
+      if (static_cast<int>(threadIdx.x) < h) {
+        red[0][threadIdx.x] += red[0][threadIdx.x + h];
+        red[1][threadIdx.x] += red[1][threadIdx.x + h];
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0 && dotp) {
+      dotp[2 * b] = red[0][0];
+      dotp[2 * b + 1] = red[1][0];
+    }
+  }
 }
 
 int g_num_sms = 0;
@@ -183,6 +350,7 @@ int g_num_sms = 0;
 }  // namespace
 
 size_t hv_rows_smem_bytes(const DevSector& S) {
+  if (S.dn_ent4) return static_cast<size_t>(S.Dd + 8) * sizeof(double2);
   return static_cast<size_t>(S.Dd) * sizeof(double2) + static_cast<size_t>(S.n_dn_hops + 1) * 8 * sizeof(double2);
 }
 
@@ -200,29 +368,39 @@ void init_sm_count() {
 }
 
 template <int kThreads>
-cudaError_t launch_cols(const DevSector& S, const double2* x, double2* y, cudaStream_t st) {
+cudaError_t launch_cols(const DevSector& S, const double2* x, double2* y, cudaStream_t st, double sx, double* dotp) {
   const int64_t nchunks = (S.Dd + 2 * kThreads - 1) / (2 * kThreads);
-  hv_cols_kernel<kThreads><<<static_cast<unsigned>(nchunks * S.Du), kThreads, 0, st>>>(S, x, y);
+  const unsigned grid = static_cast<unsigned>(nchunks * S.Du);
+  if (dotp || sx != 1.0)
+    hv_cols_kernel<kThreads, true><<<grid, kThreads, 0, st>>>(S, x, y, sx, dotp);
+  else
+    hv_cols_kernel<kThreads, false><<<grid, kThreads, 0, st>>>(S, x, y, sx, dotp);
   return cudaGetLastError();
 }
 
+int64_t hv_cols_blocks(const DevSector& S, int cols_variant) {
+  const int threads = cols_variant == 1 ? 64 : (cols_variant == 2 ? 256 : 128);
+  return (S.Dd + 2 * threads - 1) / (2 * threads) * S.Du;
+}
+
 cudaError_t hv_launch_pass(const DevSector& S, const double2* x, double2* y, int pass, cudaStream_t st,
-                           int cols_variant) {
+                           int cols_variant, double sx, double* dotp) {
   if (S.dim <= 0) return cudaSuccess;
   init_sm_count();
   if (pass == 0) {
     cudaError_t e = cudaMemsetAsync(S.flags, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
     const size_t sm = hv_rows_smem_bytes(S);
-    e = cudaFuncSetAttribute(hv_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
+    const RowsKernel k = S.dn_ent4 ? rows_compact(S.dn_re_bits, S.dn_im_bits) : hv_rows_kernel;
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
     if (e != cudaSuccess) return e;
     const int grid_r = static_cast<int>(std::min<int64_t>(S.Du, g_num_sms));
-    hv_rows_kernel<<<grid_r, kRowThreads, sm, st>>>(S, x, y);
+    k<<<grid_r, kRowThreads, sm, st>>>(S, x, y, sx);
     return cudaGetLastError();
   }
-  if (cols_variant == 1) return launch_cols<64>(S, x, y, st);
-  if (cols_variant == 2) return launch_cols<256>(S, x, y, st);
-  return launch_cols<128>(S, x, y, st);
+  if (cols_variant == 1) return launch_cols<64>(S, x, y, st, sx, dotp);
+  if (cols_variant == 2) return launch_cols<256>(S, x, y, st, sx, dotp);
+  return launch_cols<128>(S, x, y, st, sx, dotp);
 }
 
 cudaError_t hv_launch(const DevSector& S, const double2* x, double2* y, int path, cudaStream_t st, int cols_variant) {

@@ -12,8 +12,11 @@ namespace ftlm_b200 {
 cudaError_t hv_launch(const DevSector& S, const double2* x, double2* y, int path, cudaStream_t st,
                       int cols_variant = 0);
 // One pass of the fast path: 0 = row pass (diag + down hops), 1 = column-slab pass (up hops).
+// sx: the passes compute H (sx x) (sx = 1: plain H x, unchanged arithmetic); dotp (column pass,
+// may be null): one (re, im) partial of <sx x, y> per column-pass block, hv_cols_blocks() of them.
 cudaError_t hv_launch_pass(const DevSector& S, const double2* x, double2* y, int pass, cudaStream_t st,
-                           int cols_variant = 0);
+                           int cols_variant = 0, double sx = 1.0, double* dotp = nullptr);
+int64_t hv_cols_blocks(const DevSector& S, int cols_variant);
 bool hv_fast_path_ok(const DevSector& S, int max_up_deg);
 size_t hv_rows_smem_bytes(const DevSector& S);
 
@@ -27,6 +30,12 @@ constexpr int kResNw2 = 2 * kRedBlocks + 2; // ||w||^2
 constexpr int kResN0 = 2 * kRedBlocks + 3;  // ||q||^2 (start vector)
 
 cudaError_t lz_dotc(const double2* q, const double2* w, int64_t n, double* scratch, cudaStream_t st);
+// Sum of nb (re, im) partials (fixed two-level tree) into scratch[kResZ..kResZ+1].
+cudaError_t lz_reduce_pairs(const double* partial, int64_t nb, double* scratch, cudaStream_t st);
+// Lanczos update on unnormalised vectors q_k = sk Wk, q_{k-1} = skm1 Wkm1:
+// w = w - z q_k - bprev q_{k-1} (z from scratch[kResZ]); ||w||^2 -> scratch[kResNw2].
+cudaError_t lz_update_scaled(double2* w, const double2* Wk, double sk, const double2* Wkm1, double skm1, double bprev,
+                             int use_prev, int64_t n, double* scratch, cudaStream_t st);
 // w = w - z q - bprev * qp (bprev from host; use_prev selects the second term); ||w||^2 -> scratch.
 cudaError_t lz_update(double2* w, const double2* q, const double2* qp, double bprev, int use_prev, int64_t n,
                       double* scratch, cudaStream_t st);

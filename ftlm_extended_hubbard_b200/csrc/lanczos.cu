@@ -86,6 +86,53 @@ __global__ void __launch_bounds__(kRedThreads) update_kernel(double2* __restrict
   if (threadIdx.x == 0) partial[blockIdx.x] = v[0];
 }
 
+// Lanczos update with the scales of the unnormalised vectors applied on the fly.
+__global__ void __launch_bounds__(kRedThreads) update_scaled_kernel(double2* __restrict__ w,
+                                                                    const double2* __restrict__ Wk, double sk,
+                                                                    const double2* __restrict__ Wkm1, double skm1,
+                                                                    const double* __restrict__ zp, double bprev,
+                                                                    int use_prev, int64_t n,
+                                                                    double* __restrict__ partial) {
+  __shared__ double sh[kRedThreads];
+  const double zr = zp[0], zi = zp[1];
+  double v[1] = {0.0};
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * kRedThreads;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * kRedThreads + threadIdx.x; i < n; i += stride) {
+    double2 a = w[i];
+    const double2 b0 = Wk[i];
+    const double bx = sk * b0.x, by = sk * b0.y;
+    a.x -= zr * bx - zi * by;
+    a.y -= zr * by + zi * bx;
+    if (use_prev) {
+      const double2 c = Wkm1[i];
+      a.x -= bprev * (skm1 * c.x);
+      a.y -= bprev * (skm1 * c.y);
+    }
+    w[i] = a;
+    v[0] += a.x * a.x + a.y * a.y;
+  }
+  block_sum<1>(v, sh);
+  if (threadIdx.x == 0) partial[blockIdx.x] = v[0];
+}
+
+// First level of a pair reduction: block b sums pairs [b*per, (b+1)*per) in order.
+__global__ void __launch_bounds__(kRedThreads) pairs_kernel(const double* __restrict__ in, int64_t nb, int64_t per,
+                                                            double* __restrict__ out) {
+  __shared__ double sh[2 * kRedThreads];
+  double v[2] = {0.0, 0.0};
+  const int64_t b0 = static_cast<int64_t>(blockIdx.x) * per;
+  const int64_t b1 = min(nb, b0 + per);
+  for (int64_t i = b0 + threadIdx.x; i < b1; i += kRedThreads) {
+    v[0] += in[2 * i];
+    v[1] += in[2 * i + 1];
+  }
+  block_sum<2>(v, sh);
+  if (threadIdx.x == 0) {
+    out[2 * blockIdx.x] = v[0];
+    out[2 * blockIdx.x + 1] = v[1];
+  }
+}
+
 __global__ void scale_kernel(double2* __restrict__ dst, const double2* __restrict__ src, int64_t n,
                              const double* __restrict__ nw2) {
   const double b = sqrt(*nw2);
@@ -160,6 +207,21 @@ cudaError_t lz_dotc(const double2* q, const double2* w, int64_t n, double* scrat
 cudaError_t lz_update(double2* w, const double2* q, const double2* qp, double bprev, int use_prev, int64_t n,
                       double* scratch, cudaStream_t st) {
   update_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(w, q, qp, scratch + kResZ, bprev, use_prev, n, scratch);
+  final_kernel<1><<<1, kRedThreads, 0, st>>>(scratch, kRedBlocks, scratch + kResNw2);
+  return cudaGetLastError();
+}
+
+cudaError_t lz_reduce_pairs(const double* partial, int64_t nb, double* scratch, cudaStream_t st) {
+  const int64_t per = (nb + kRedBlocks - 1) / kRedBlocks;
+  pairs_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(partial, nb, per, scratch);
+  final_kernel<2><<<1, kRedThreads, 0, st>>>(scratch, kRedBlocks, scratch + kResZ);
+  return cudaGetLastError();
+}
+
+cudaError_t lz_update_scaled(double2* w, const double2* Wk, double sk, const double2* Wkm1, double skm1, double bprev,
+                             int use_prev, int64_t n, double* scratch, cudaStream_t st) {
+  update_scaled_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(w, Wk, sk, Wkm1, skm1, scratch + kResZ, bprev, use_prev, n,
+                                                          scratch);
   final_kernel<1><<<1, kRedThreads, 0, st>>>(scratch, kRedBlocks, scratch + kResNw2);
   return cudaGetLastError();
 }

@@ -151,6 +151,71 @@ void schedule_quarter(const std::vector<uint32_t>* in, std::vector<uint32_t>* ou
   }
 }
 
+// Index of v in the class list (appended when new and there is room), or -1.
+int class_of(double v, double* list, int* n) {
+  for (int i = 0; i < *n; ++i)
+    if (list[i] == v) return i;
+  if (*n >= 4) return -1;
+  list[*n] = v;
+  return (*n)++;
+}
+
+int bits_for(int n) { return n <= 1 ? 0 : (n <= 2 ? 1 : 2); }
+
+// The compact row-pass table (see SectorPlan::dn_compact): the entries of dn_ent re-encoded with
+// the hop's sites and coefficient classes instead of its id.
+void build_compact_down(SectorPlan* Pp) {
+  SectorPlan& P = *Pp;
+  P.dn_compact = false;
+  P.dn_gptr4.clear();
+  P.dn_ent4.clear();
+  const int64_t Dd = P.dn.D;
+  if (P.n > 31 || Dd + 8 > (1 << 14) || P.dn_gptr.size() < 2) return;
+  const int nh = static_cast<int>(P.hd.size());
+  std::vector<uint32_t> code(static_cast<size_t>(nh) + 1, 0u);
+  int nre = 0, nim = 0;
+  for (int h = 0; h < nh; ++h) {
+    const MergedHop& m = P.hd[static_cast<size_t>(h)];
+    const int kr = class_of(m.cre, P.dn_re, &nre);
+    const int ki = class_of(std::fabs(m.cim), P.dn_im, &nim);
+    if (kr < 0 || ki < 0) return;
+    code[static_cast<size_t>(h)] = (static_cast<uint32_t>(m.lo + 1) << 14) | (static_cast<uint32_t>(m.hi + 1) << 19) |
+                                   (static_cast<uint32_t>(kr) << 25) | (static_cast<uint32_t>(ki) << 27) |
+                                   (static_cast<uint32_t>(std::signbit(m.cim) ? 1 : 0) << 29);
+  }
+  P.dn_re_bits = bits_for(nre);
+  P.dn_im_bits = (nim <= 1 && P.dn_im[0] == 0.0) ? -1 : bits_for(nim);
+  auto sentinel = [Dd](uint32_t group) {
+    return static_cast<uint32_t>(Dd + static_cast<int64_t>((group + 8 - static_cast<uint32_t>(Dd & 7)) & 7));
+  };
+  const int64_t ngroups = static_cast<int64_t>(P.dn_gptr.size()) - 1;
+  P.dn_gptr4.assign(static_cast<size_t>(ngroups) + 1, 0);
+  for (int64_t g = 0; g < ngroups; ++g) {
+    const int64_t base = P.dn_gptr[static_cast<size_t>(g)];
+    const int64_t K = (P.dn_gptr[static_cast<size_t>(g) + 1] - base) / 32;
+    const int64_t K4 = (K + 3) / 4 * 4;
+    const size_t off = P.dn_ent4.size();
+    P.dn_ent4.resize(off + static_cast<size_t>(K4) * 32, 0u);
+    for (int64_t k = 0; k < K4; ++k)
+      for (uint32_t l = 0; l < 32; ++l) {
+        uint32_t out;
+        if (k < K) {
+          const uint32_t e = P.dn_ent[static_cast<size_t>(base + 32 * k + l)];
+          const uint32_t src = e >> 10, h = (e >> 1) & 511u;
+          if (static_cast<int>(h) == P.dn_pad_hop)
+            out = sentinel(src & 7u);  // zero element in the same bank group: zero contribution
+          else
+            out = src | code[h] | ((e & 1u) << 24);
+        } else {
+          out = sentinel(l & 7u);  // extra rounds: the 8 lanes of a quarter hit 8 distinct groups
+        }
+        P.dn_ent4[off + static_cast<size_t>(((k / 4) * 32 + l) * 4 + (k % 4))] = out;
+      }
+    P.dn_gptr4[static_cast<size_t>(g) + 1] = static_cast<int64_t>(P.dn_ent4.size());
+  }
+  P.dn_compact = true;
+}
+
 }  // namespace
 
 uint64_t binom(int n, int k) {
@@ -397,6 +462,7 @@ std::string build_plan(int n_sites, int n_up, int n_dn, double U, double V, cons
     P.dn_gptr[static_cast<size_t>(g) + 1] = static_cast<int64_t>(P.dn_ent.size());
   }
   P.mean_dn_sources = P.dn.D ? static_cast<double>(total_src) / static_cast<double>(P.dn.D) : 0.0;
+  build_compact_down(&P);
   return "";
 }
 

@@ -82,6 +82,19 @@ struct SectorPlan {
   std::vector<double> dn_coef;     // 2 per hop id (pad hop id has 0)
   std::vector<uint32_t> dn_nmask;  // per hop id
 
+  // Compact row-pass table (same entries and order as dn_ent), built when the merged down-hop
+  // coefficients take at most 4 distinct real parts and 4 distinct |imaginary parts|,
+  // Dd + 8 <= 16384 and n_sites <= 31.  Entry = src | (lo+1)<<14 | (hi+1)<<19 | dn_sign<<24 |
+  // re_class<<25 | im_class<<27 | im_negative<<29; the per-row up-string factor is
+  // parity(u in (lo, hi]) from the up string's prefix parity; src >= Dd addresses one of 8 zero
+  // sentinels after the staged row (padding, one per bank group).  Rounds are padded to a multiple
+  // of 4 and stored [group][round/4][lane][4] so that a lane loads 4 entries with one 16-byte load.
+  bool dn_compact = false;
+  int dn_re_bits = 0, dn_im_bits = 0;  // class-index widths (0, 1 or 2); dn_im_bits = -1: all real
+  double dn_re[4] = {0, 0, 0, 0}, dn_im[4] = {0, 0, 0, 0};
+  std::vector<int64_t> dn_gptr4;  // per group, offset in entries (multiple of 128)
+  std::vector<uint32_t> dn_ent4;
+
   double mean_up_sources = 0.0, mean_dn_sources = 0.0;
   int max_dn_deg = 0, max_up_deg = 0;
 };

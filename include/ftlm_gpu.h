@@ -94,6 +94,14 @@ int ftlm_gpu_sector_stats(const ftlm_sector* s, double* mean_up_sources, double*
  * query the sizes. */
 int ftlm_gpu_sector_down_table(const ftlm_sector* s, long long* n_groups, long long* n_entries, long long* gptr,
                                uint32_t* entries, int* pad_hop);
+/* Host copy of the compact row-pass table (inspection and tests; no reference counterpart):
+ * *available = 0 when the sector's down hops do not fit its coefficient classes.  Entries
+ * src | (lo+1)<<14 | (hi+1)<<19 | dn_sign<<24 | re_class<<25 | im_class<<27 | im_negative<<29,
+ * stored [group][round/4][lane][4]; src >= Dd is a zero sentinel (padding).  re4/im4 receive the
+ * 4 real parts and |imaginary parts| the classes index.  NULL buffers query the sizes. */
+int ftlm_gpu_sector_down_table_compact(const ftlm_sector* s, int* available, long long* n_groups,
+                                       long long* n_entries, long long* gptr, uint32_t* entries, double* re4,
+                                       double* im4, int* re_bits, int* im_bits);
 /* Diagonal entry H[i,i] (host computation from the sector tables). */
 int ftlm_gpu_sector_diag(const ftlm_sector* s, long long index, double* value);
 
@@ -105,7 +113,11 @@ int ftlm_gpu_apply_host(ftlm_sector* s, const double* x_host, double* y_host);
  * = row pass, column-slab pass (one entry for the generic path); *n_passes = entries written. */
 int ftlm_gpu_apply_profiled(ftlm_sector* s, const double* x_dev, double* y_dev, void* stream, float* ms_passes,
                             int* n_passes);
-/* Kernel selection for ftlm_gpu_apply: 0 = automatic, 1 = generic gather, 2 = row+slab passes. */
+/* Kernel selection for ftlm_gpu_apply: 0 = automatic, 1 = generic gather, 2 = row+slab passes
+ * (row pass with a per-row coefficient table in shared memory), 3 = row+slab passes with the row
+ * pass reading register-held coefficient classes from a compact entry table (sectors whose down hops
+ * take at most 4 distinct real and 4 distinct |imaginary| coefficient parts; else as 2).  2 and 3
+ * give the same sums. */
 int ftlm_gpu_set_apply_path(ftlm_sector* s, int path);
 
 /* lanczos_tridiagonal on the sector operator.  alpha/beta: host arrays of max_steps entries;
@@ -160,6 +172,14 @@ int ftlm_gpu_ritz_values(const double* alpha, const double* beta, int n, int k, 
 int ftlm_gpu_ftlm_sector(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed, int start_mode,
                          double* lnz, double* energy);
 
+/* Quadrature of the complex128 sector path (ftlm_gpu_ftlm_sector, ftlm_gpu_gc_sweep, orbit blocks):
+ * FTLM_QUAD_REFERENCE (default) = the reference's classical Jacobi with max(3000, 120 n) rotations
+ * (src/ftlm_thermo.cpp:83-146; for n ~ 100 at low temperature it stops unconverged, so its ln Z moves
+ * by up to ~1e-5 under 1e-7 changes of alpha/beta); FTLM_QUAD_CONVERGED = the converged GPU Jacobi.
+ * The batched complex64 path always uses the converged quadrature.  Process-wide setting. */
+#define FTLM_QUAD_REFERENCE 0
+#define FTLM_QUAD_CONVERGED 1
+int ftlm_gpu_set_quadrature(int mode);
 /* Sector ln Z from R chain quadratures (src/ftlm_thermo.cpp:246-256): lnz[b] = log_dim +
  * log mean_{r: used[r] > 0} e^{logq[r][b]}; energy = e^{logq}-weighted chain energies.  Host arrays. */
 int ftlm_gpu_ftlm_combine(const double* logq, const double* energy_r, const int* used, int R, int n_bt, double log_dim,
@@ -185,13 +205,29 @@ int ftlm_gpu_gc_sweep(const ftlm_params* p, int R, int M, unsigned seed, int sta
 /* alpha/beta [R][M] (beta zero-padded after a breakdown), used [R]. */
 int ftlm_gpu_batched_lanczos(ftlm_sector* s, int R, int M, unsigned seed, double* alpha, double* beta, int* used);
 /* ftlm_gpu_ftlm_sector on the batched path; sectors with dim <= 2M use the complex128 path with
- * FTLM_START_PHILOX (their Krylov space can be exhausted, where FP64 breakdown detection matters). */
+ * FTLM_START_PHILOX (their Krylov space can be exhausted, where FP64 breakdown detection matters).
+ * Chains are evaluated with the converged quadrature (FTLM_QUAD_CONVERGED). */
 int ftlm_gpu_batched_ftlm_sector(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed, double* lnz,
                                  double* energy);
+/* ftlm_gpu_batched_ftlm_sector with its rounding-error estimate against the complex128 path (the
+ * per-result error statement of the complex64 method; no reference counterpart): chains r < n_check
+ * (n_check >= 1) are rerun with complex128 vectors from the same Philox start and
+ * lnz_err[b] = max_r |L_r(complex64) - L_r(complex128)|, L_r the chain's log quadrature at bts[b];
+ * it bounds |d ln Z| for a common per-chain error.  Sectors on the complex128 path report 0. */
+int ftlm_gpu_batched_ftlm_sector_checked(ftlm_sector* s, const double* bts, int n_bt, int R, int M, unsigned seed,
+                                         int n_check, double* lnz, double* energy, double* lnz_err);
 /* ftlm_gpu_gc_sweep on the batched path (config: all sectors, R chains, M steps). */
 int ftlm_gpu_batched_sweep(const ftlm_params* p, int R, int M, unsigned seed, const double* bts, int n_bt,
                            const double* mus, int n_mu, double* lnz_s, double* e_s, double* lnz_gc, double* n_avg,
                            double* e_avg);
+/* ftlm_gpu_batched_sweep with per-result error estimates against the complex128 path: lnz_s_err
+ * [n_sec][n_bt] as ftlm_gpu_batched_ftlm_sector_checked, and their first-order propagation through
+ * the grand-canonical combination, lnz_gc_err = sum_s w_s lnz_s_err and n_err = sum_s w_s
+ * |N_s/n - <n>| lnz_s_err ([n_bt][n_mu], w_s the sector weights).  n_check >= 1 complex128 chains
+ * per sector (about n_check/R of the plain path's cost). */
+int ftlm_gpu_batched_sweep_checked(const ftlm_params* p, int R, int M, unsigned seed, const double* bts, int n_bt,
+                                   const double* mus, int n_mu, int n_check, double* lnz_s, double* e_s, double* lnz_gc,
+                                   double* n_avg, double* e_avg, double* lnz_s_err, double* lnz_gc_err, double* n_err);
 int ftlm_gpu_batched_release(void);
 
 /* Sectors with 2 <= dim <= max_dim in ftlm_gpu_gc_sweep run as one fused launch (one CTA per chain,
@@ -199,7 +235,8 @@ int ftlm_gpu_batched_release(void);
  * No reference counterpart (scheduling only). */
 int ftlm_gpu_set_fused_max_dim(long long max_dim);
 /* Autotuner (no reference counterpart): times the sector's H·v variants — the generic gather kernel
- * and, where it fits, the row + column-slab pair with 256-, 128- and 512-column slabs — `reps` times
+ * and, where it fits, the row + column-slab pair with 256-, 128- and 512-column slabs (and the
+ * register-class row pass with 256-column slabs) — `reps` times
  * each on a device vector and keeps the fastest for this handle (later ftlm_gpu_apply calls use it).
  * The choice is cached per sector shape (sites, particle numbers, hop counts) for the process; a
  * cached answer returns *ms = -1.  Outputs may be NULL.  Replaces ftlm_gpu_set_apply_path's choice. */
