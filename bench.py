@@ -57,6 +57,10 @@ def parse():
                          "grand-canonical sweep, batched complex64 and plain complex128 (same Philox starts), "
                          "R=32, M=100, T=0.1..2 x mu=-4..8 (tens of minutes)")
     ap.add_argument("--k", type=int, nargs=2, default=(1, 2), metavar=("KX", "KY"), help="orbit workload momentum")
+    ap.add_argument("--hv-path", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="hv workload: pin the H·v kernel path (0 = the autotuner's choice)")
+    ap.add_argument("--cols-variant", type=int, default=0, choices=[0, 1, 2],
+                    help="with --hv-path: column-slab width variant (0/1/2 = 256/128/512 columns)")
     ap.add_argument("--check", type=int, default=1,
                     help="sweep workload: chains per sector rerun in complex128 for the per-result error estimate")
     return ap.parse_args()
@@ -259,7 +263,13 @@ def run_ours(args):
     p = F.HubbardParams(**PARAMS)
     nu, nd = args.sector if args.sector else (NU, ND)
     sec = F.Sector(p, nu, nd)
-    tuned_path, tuned_cols, _ = sec.autotune(3)  # project autotuner: H·v variant for this sector shape
+    if args.hv_path:
+        sec.set_apply_path(args.hv_path)
+        call("ftlm_gpu_set_cols_variant", sec.handle, args.cols_variant)
+        tuned_path, tuned_cols, chosen_by = args.hv_path, args.cols_variant, "command line"
+    else:
+        tuned_path, tuned_cols, _ = sec.autotune(3)  # project autotuner: H·v variant for this sector shape
+        chosen_by = "autotuner"
     st = sec.stats()
     dim = sec.dim()
     g = torch.Generator(device="cuda")
@@ -350,13 +360,14 @@ def run_ours(args):
                    "vector": "torch.randn complex128, seed 7+rank",
                    "l2": "inputs larger than L2 (2.65 GB per vector); no flush",
                    "parallelism": f"independent H·v per rank x{ws}",
-                   "hv_variant": {"path": tuned_path, "cols_slab": [256, 128, 512][tuned_cols], "chosen_by": "autotuner"}},
+                   "hv_variant": {"path": tuned_path, "cols_slab": [256, 128, 512][tuned_cols], "chosen_by": chosen_by}},
         "gpu_launches": 2 * args.steps,
         "kernels_ms": {"hv_rows": rows_avg, "hv_cols": cols_avg},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": read_profile_traffic(dom) if not args.sector else None,
                      "algorithmic_bytes_per_launch": alg[dom], "peak_source": peak_src,
-                     "peak_note": "hbm_gbs of MEASURED_PEAKS.json (burst copy)",
+                     "peak_note": ("hbm_gbs of MEASURED_PEAKS.json (burst copy)" if peaks else
+                                   "fallback: MEASURED_PEAKS.json absent; 6650 GB/s, an earlier STREAM-style copy on B200"),
                      "hv_model_frac": hv_bytes / (ms_max / args.steps / 1000.0) / 1e9 / hbm,
                      "compulsory_frac": 2 * c * dim / (ms_max / args.steps / 1000.0) / 1e9 / hbm},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(dim * 16), "d2h_bytes_per_step": int(dim * 16),

@@ -72,7 +72,7 @@ SIGNATURES = {
     "ftlm_gpu_sector_stats": [_vp, _pd, _pd, C.POINTER(_ll), C.POINTER(_ll)],
     "ftlm_gpu_sector_diag": [_vp, _ll, _pd],
     "ftlm_gpu_sector_down_table": [_vp, C.POINTER(_ll), C.POINTER(_ll), _vp, _vp, _pi],
-    "ftlm_gpu_sector_down_table_compact": [_vp, _pi, C.POINTER(_ll), C.POINTER(_ll), _vp, _vp, _vp, _vp, _pi, _pi],
+    "ftlm_gpu_sector_down_table_gauge": [_vp, _pi, C.POINTER(_ll), C.POINTER(_ll), _pi, _vp, _vp, _vp, _vp],
     "ftlm_gpu_apply": [_vp, _vp, _vp, _vp],
     "ftlm_gpu_apply_host": [_vp, _vp, _vp],
     "ftlm_gpu_apply_profiled": [_vp, _vp, _vp, _vp, C.POINTER(C.c_float), _pi],
@@ -87,6 +87,8 @@ SIGNATURES = {
     "ftlm_gpu_ftlm_sector": [_vp, _vp, _i, _i, _i, C.c_uint, _i, _vp, _vp],
     "ftlm_gpu_gc_reduce": [_vp, _vp, _vp, _i, _vp, _i, _vp, _i, _i, _vp, _vp, _vp],
     "ftlm_gpu_batched_lanczos": [_vp, _i, _i, C.c_uint, _vp, _vp, _vp],
+    "ftlm_gpu_batched_set_cols_variant": [_vp, _i],
+    "ftlm_gpu_batched_autotune": [_vp, _i, _vp, _vp],
     "ftlm_gpu_batched_ftlm_sector": [_vp, _vp, _i, _i, _i, C.c_uint, _vp, _vp],
     "ftlm_gpu_batched_sweep": [C.POINTER(FtlmParams), _i, _i, C.c_uint, _vp, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp],
     "ftlm_gpu_batched_release": [],

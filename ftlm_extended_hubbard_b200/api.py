@@ -270,6 +270,17 @@ class Sector(_Handle):
         return lnz, en
 
 
+    def batched_set_cols_variant(self, variant: int):
+        """Column-pass variant of the batched H·v: 0/1/2 = 16/8/4-column chunks."""
+        call("ftlm_gpu_batched_set_cols_variant", self._h, variant)
+
+    def batched_autotune(self, reps: int = 2):
+        """Time the batched column-pass variants and keep the fastest: (variant, ms per block H·v;
+        -1 when the shape's answer was cached)."""
+        var, ms = C.c_int(), C.c_float()
+        call("ftlm_gpu_batched_autotune", self._h, reps, C.byref(var), C.byref(ms))
+        return var.value, ms.value
+
     def batched_lanczos(self, n_random: int, lanczos_steps: int, seed: int):
         """32-chain complex64 Lanczos: alpha/beta [R][M] (beta zero-padded), used [R]."""
         R, M = n_random, lanczos_steps

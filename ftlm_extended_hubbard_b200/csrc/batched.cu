@@ -237,13 +237,13 @@ __device__ __forceinline__ float4 bt_cols_sum(const float4* Wc, const uint32_t* 
 
 // Column pass (gauge basis): Y[r, c, :] += sum_j u_j W[src_j, c, :] with the coefficients u_j of
 // output up string r the same for every column (the down string no longer enters the sign), then
-// the fused <W_k, Y> per chain.  Work item = (16-column chunk, output row r), walked chunk-major by
-// a persistent grid so that the chunk's slab of W (Du x 16 x 256 bytes) stays in L2; in an item,
-// thread (column t/16, lane t%16) owns chains 2l, 2l+1 of one column and every source row is read
-// as one contiguous 4-kilobyte segment.  Each block keeps its items' dot sums in registers and
-// writes one partial per chain (fixed work order: bitwise repeatable).
-constexpr int kBgCols = 16;
-
+// the fused <W_k, Y> per chain.  Work item = (kCols-column chunk, group of kRows output rows), walked
+// chunk-major by a persistent grid so that the chunk's slab of W (Du x kCols x 256 bytes) stays in
+// L2; in an item, thread (row t / (16 kCols), column t / 16 % kCols, lane t % 16) owns chains 2l,
+// 2l+1 of one element and every source row is read as one contiguous kCols x 256-byte segment.
+// kCols = 16 / 8 / 4 (slabs of 52.7 / 26.4 / 13.2 MB at 4x4 (8,8)) are the variants the batched
+// autotuner chooses from.  Each block keeps its items' dot sums in registers and writes one partial
+// per chain (fixed work order: bitwise repeatable for a given variant).
 template <bool kFilter>
 __device__ __forceinline__ float4 bg_cols_sum(const float4* __restrict__ Wc, const uint32_t* s_off,
                                               const float2* s_cf, int deg) {
@@ -263,38 +263,48 @@ __device__ __forceinline__ float4 bg_cols_sum(const float4* __restrict__ Wc, con
   return acc;
 }
 
+template <int kCols>
 __global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_cols_kernel(DevSector S, const float2* __restrict__ W,
                                                                              float2* __restrict__ Y,
                                                                              double* __restrict__ partial,
                                                                              const int* __restrict__ flag) {
-  __shared__ uint32_t s_off[kMaxUpDegB];
-  __shared__ float2 s_cf[kMaxUpDegB];
+  constexpr int kRows = kBtThreads / (16 * kCols);
+  __shared__ uint32_t s_off[kRows][kMaxUpDegB];
+  __shared__ float2 s_cf[kRows][kMaxUpDegB];
   __shared__ double sh[4 * kBtThreads];
   const int t = threadIdx.x;
-  const int col = t >> 4, l = t & 15;
+  const int ri = t / (16 * kCols), col = (t >> 4) % kCols, l = t & 15;
   const bool filter = *flag != 0;
   const int Dd = static_cast<int>(S.Dd), Du = static_cast<int>(S.Du);
   const uint32_t row_stride = static_cast<uint32_t>(Dd) * 16u;  // float4 units per row
   const float4* W4 = reinterpret_cast<const float4*>(W);
   float4* Y4 = reinterpret_cast<float4*>(Y);
-  const int64_t nchunks = (Dd + kBgCols - 1) / kBgCols;
-  const int64_t items = nchunks * Du;
+  const int64_t nchunks = (Dd + kCols - 1) / kCols;
+  const int64_t ngroups = (Du + kRows - 1) / kRows;
+  const int64_t items = nchunks * ngroups;
   double d0r = 0.0, d0i = 0.0, d1r = 0.0, d1i = 0.0;  // chains 2l and 2l+1
   for (int64_t it = blockIdx.x; it < items; it += gridDim.x) {
-    const int64_t chunk = it / Du;
-    const int r = static_cast<int>(it - chunk * Du);
-    const int j0 = S.up_ptr[r];
-    const int deg = S.up_ptr[r + 1] - j0;
-    __syncthreads();  // the previous item's list is no longer read
-    for (int j = t; j < deg; j += kBtThreads) {
-      s_off[j] = static_cast<uint32_t>(S.up_src[j0 + j]) * row_stride;
-      s_cf[j] = S.up_coef32[j0 + j];
+    const int64_t chunk = it / ngroups;
+    const int r0 = static_cast<int>(it - chunk * ngroups) * kRows;
+    __syncthreads();  // the previous item's lists are no longer read
+#pragma unroll
+    for (int q = 0; q < kRows; ++q) {
+      if (r0 + q >= Du) break;
+      const int j0 = S.up_ptr[r0 + q];
+      const int dq = S.up_ptr[r0 + q + 1] - j0;
+      for (int j = t; j < dq; j += kBtThreads) {
+        s_off[q][j] = static_cast<uint32_t>(S.up_src[j0 + j]) * row_stride;
+        s_cf[q][j] = S.up_coef32[j0 + j];
+      }
     }
     __syncthreads();
-    const int c = static_cast<int>(chunk) * kBgCols + col;
-    if (c < Dd) {
+    const int r = r0 + ri;
+    const int c = static_cast<int>(chunk) * kCols + col;
+    if (r < Du && c < Dd) {
+      const int deg = S.up_ptr[r + 1] - S.up_ptr[r];
       const float4* Wc = W4 + static_cast<uint32_t>(c) * 16u + l;
-      const float4 acc = filter ? bg_cols_sum<true>(Wc, s_off, s_cf, deg) : bg_cols_sum<false>(Wc, s_off, s_cf, deg);
+      const float4 acc = filter ? bg_cols_sum<true>(Wc, s_off[ri], s_cf[ri], deg)
+                                : bg_cols_sum<false>(Wc, s_off[ri], s_cf[ri], deg);
       const int64_t o = static_cast<int64_t>(r) * row_stride + static_cast<uint32_t>(c) * 16u + l;
       float4 y = Y4[o];
       y.x += acc.x;
@@ -312,7 +322,7 @@ __global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_cols_kernel(Dev
       d1i = fma(wz, yw, fma(-ww, yz, d1i));
     }
   }
-  // per-chain block sums: thread t holds chains 2l, 2l+1 of column t/16
+  // per-chain block sums: thread t holds chains 2l, 2l+1 of one element
   sh[0 * kBtThreads + t] = d0r;
   sh[1 * kBtThreads + t] = d0i;
   sh[2 * kBtThreads + t] = d1r;
@@ -329,6 +339,17 @@ __global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_cols_kernel(Dev
     partial[(blockIdx.x * 32 + chain) * 2] = re;
     partial[(blockIdx.x * 32 + chain) * 2 + 1] = im;
   }
+}
+
+cudaError_t launch_bt_cols(int cols_variant, const DevSector& S, const float2* W, float2* Y, double* partial,
+                           const int* flag, cudaStream_t s) {
+  if (cols_variant == 1)
+    bt_cols_kernel<8><<<kBtBlocks, kBtThreads, 0, s>>>(S, W, Y, partial, flag);
+  else if (cols_variant == 2)
+    bt_cols_kernel<4><<<kBtBlocks, kBtThreads, 0, s>>>(S, W, Y, partial, flag);
+  else
+    bt_cols_kernel<16><<<kBtBlocks, kBtThreads, 0, s>>>(S, W, Y, partial, flag);
+  return cudaGetLastError();
 }
 
 // W_{k+1} = s_in Y - c1 W_k - c2 W_{k-1} (in Y's buffer, FP64 then rounded), ||W_{k+1}||^2 partials per chain.
@@ -586,7 +607,7 @@ cudaError_t bt_step(const DevSector& S, const float2* Wk, const float2* Wkm1, fl
   cudaError_t e = cudaMemsetAsync(fout, 0, sizeof(int), s);
   if (e != cudaSuccess) return e;
   bt_rows_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(S, Wk, Y, fin);
-  bt_cols_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(S, Wk, Y, partial, fin);
+  launch_bt_cols(S.bt_cols, S, Wk, Y, partial, fin, s);
   bt_scalar_kernel<<<1, 32, 0, s>>>(partial, kBtBlocks, 1, k, st, alpha, beta, used);
   bt_update_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(Y, Wk, Wkm1, S.dim, st, k > 0, partial, fout);
   bt_scalar_kernel<<<1, 32, 0, s>>>(partial, kBtBlocks, 2, k, st, alpha, beta, used);
@@ -610,7 +631,7 @@ cudaError_t bt_apply(const DevSector& S, const float2* X, float2* Y, const doubl
                      const int* zero_flag, cudaStream_t s) {
   (void)st_unit;
   bt_rows_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(S, X, Y, zero_flag);
-  bt_cols_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(S, X, Y, partial, zero_flag);
+  launch_bt_cols(S.bt_cols, S, X, Y, partial, zero_flag, s);
   return cudaGetLastError();
 }
 

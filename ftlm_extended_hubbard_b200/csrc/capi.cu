@@ -115,22 +115,28 @@ int upload_plan(ftlm_sector* s) {
   std::vector<int> flags(4, 0);
   int* fl;
   CU_TRY(upload(flags, &fl, &s->owned));
-  D.dn_ent4 = nullptr;
-  D.dn_gptr4 = nullptr;
-  if (P.dn_compact) {
-    uint32_t* e4;
-    int64_t* g4;
-    CU_TRY(upload(P.dn_ent4, &e4, &s->owned));
-    CU_TRY(upload(P.dn_gptr4, &g4, &s->owned));
-    D.dn_ent4 = reinterpret_cast<const uint4*>(e4);
-    D.dn_gptr4 = g4;
-    for (int i = 0; i < 4; ++i) {
-      D.dn_re[i] = P.dn_re[i];
-      D.dn_im[i] = P.dn_im[i];
+  D.bt_cols = 1;  // 8-column chunks: the fastest at 4x4 (4,4), (6,6), (8,8) (ftlm_gpu_batched_autotune)
+  auto upload_gauge = [&](const GaugeTable& G, DevGauge* out) -> cudaError_t {
+    *out = DevGauge{};
+    out->real2[0] = G.real2[0];
+    out->real2[1] = G.real2[1];
+    if (!G.ok) return cudaSuccess;
+    uint32_t* ge;
+    int32_t* gg;
+    cudaError_t e = upload(G.ent, &ge, &s->owned);
+    if (e == cudaSuccess) e = upload(G.grp, &gg, &s->owned);
+    if (e != cudaSuccess) return e;
+    out->ent = ge;
+    out->grp = reinterpret_cast<const int4*>(gg);
+    out->nt = static_cast<int>(G.tab.size() / 2);
+    if (out->nt > 0) {
+      double* gt;
+      if ((e = upload(G.tab, &gt, &s->owned)) != cudaSuccess) return e;
+      out->tab = reinterpret_cast<const double2*>(gt);
     }
-    D.dn_re_bits = P.dn_re_bits;
-    D.dn_im_bits = P.dn_im_bits;
-  }
+    return cudaSuccess;
+  };
+  CU_TRY(upload_gauge(P.dn_g, &D.dn_g));
   D.umask = um;
   D.dmask = dm;
   D.cnt_uu = cuu;
@@ -301,21 +307,19 @@ int ftlm_gpu_sector_state(const ftlm_sector* s, long long index, uint64_t* up, u
   return FTLM_OK;
 }
 
-int ftlm_gpu_sector_down_table_compact(const ftlm_sector* s, int* available, long long* n_groups,
-                                       long long* n_entries, long long* gptr, uint32_t* entries, double* re4,
-                                       double* im4, int* re_bits, int* im_bits) {
-  if (!s || !available || !n_groups || !n_entries) return fail(FTLM_ERR_INVALID, "null argument");
-  const SectorPlan& P = s->plan;
-  *available = P.dn_compact ? 1 : 0;
-  *n_groups = P.dn_compact ? static_cast<long long>(P.dn_gptr4.size()) - 1 : 0;
-  *n_entries = static_cast<long long>(P.dn_ent4.size());
-  if (!P.dn_compact) return FTLM_OK;
-  if (gptr) std::copy(P.dn_gptr4.begin(), P.dn_gptr4.end(), gptr);
-  if (entries) std::copy(P.dn_ent4.begin(), P.dn_ent4.end(), entries);
-  if (re4) std::copy(P.dn_re, P.dn_re + 4, re4);
-  if (im4) std::copy(P.dn_im, P.dn_im + 4, im4);
-  if (re_bits) *re_bits = P.dn_re_bits;
-  if (im_bits) *im_bits = P.dn_im_bits;
+int ftlm_gpu_sector_down_table_gauge(const ftlm_sector* s, int* available, long long* n_groups, long long* n_entries,
+                                     int* n_table, int* groups, uint32_t* entries, double* table, double* real2) {
+  if (!s || !available || !n_groups || !n_entries || !n_table) return fail(FTLM_ERR_INVALID, "null argument");
+  const GaugeTable& G = s->plan.dn_g;
+  *available = G.ok ? 1 : 0;
+  *n_groups = G.ok ? static_cast<long long>(G.grp.size() / 4) : 0;
+  *n_entries = G.ok ? static_cast<long long>(G.ent.size()) : 0;
+  *n_table = G.ok ? static_cast<int>(G.tab.size() / 2) : 0;
+  if (!G.ok) return FTLM_OK;
+  if (groups) std::copy(G.grp.begin(), G.grp.end(), groups);
+  if (entries) std::copy(G.ent.begin(), G.ent.end(), entries);
+  if (table) std::copy(G.tab.begin(), G.tab.end(), table);
+  if (real2) std::copy(G.real2, G.real2 + 2, real2);
   return FTLM_OK;
 }
 
@@ -982,11 +986,11 @@ int ftlm_gpu_autotune_apply(ftlm_sector* s, int reps, int* path, int* cols_varia
   int best_p = 1, best_v = 0;
   float best = 3.4e38f;
   const bool fast = hv_fast_path_ok(s->dev_for(2), P.max_up_deg);
-  const int variants[5][2] = {{1, 0}, {2, 0}, {2, 1}, {2, 2}, {3, 0}};
+  const int variants[7][2] = {{1, 0}, {2, 0}, {2, 1}, {2, 2}, {3, 0}, {3, 1}, {3, 2}};
   cudaError_t ce = cudaSuccess;
   for (const auto& v : variants) {
     if (v[0] >= 2 && !fast) continue;
-    if (v[0] == 3 && (!s->dev.dn_ent4 || hv_rows_smem_bytes(s->dev_for(3)) > 227 * 1024)) continue;
+    if (v[0] == 3 && !s->path_available(3)) continue;
     const DevSector d = s->dev_for(v[0]);
     const int lp = v[0] == 3 ? 2 : v[0];
     ce = hv_launch(d, x.as<double2>(), y.as<double2>(), lp, st, v[1]);  // warm-up

@@ -1,5 +1,7 @@
 // C ABI of the batched complex64 FTLM (batched.cu): 32 chains per block vector, the M Lanczos steps
 // of a block captured once into a CUDA graph and launched without host synchronisation.
+#include <map>
+
 #include "capi_internal.hpp"
 
 using namespace ftlm_b200;
@@ -27,6 +29,79 @@ int bt_run_chains(ftlm_sector* s, int R, int M, unsigned seed, std::vector<doubl
 }  // namespace ftlm_b200
 
 extern "C" {
+
+int ftlm_gpu_batched_set_cols_variant(ftlm_sector* s, int variant) {
+  if (!s || variant < 0 || variant > 2) return fail(FTLM_ERR_INVALID, "batched cols variant must be 0, 1 or 2");
+  s->dev.bt_cols = variant;
+  return FTLM_OK;
+}
+
+int ftlm_gpu_batched_autotune(ftlm_sector* s, int reps, int* variant, float* ms) {
+  int rc = need_device(s);
+  if (rc) return rc;
+  if (s->plan.max_up_deg > 120)
+    return fail(FTLM_ERR_UNSUPPORTED, "batched path: more than 120 up-hop sources per string");
+  reps = std::max(1, reps);
+  const SectorPlan& P = s->plan;
+  static std::mutex mu;
+  static std::map<std::string, int> cache;  // one timing per sector shape and process
+  char key[160];
+  std::snprintf(key, sizeof(key), "%d/%d/%d/%zu/%zu/%d/%d", P.n, P.nu, P.nd, P.hu.size(), P.hd.size(), P.max_up_deg,
+                P.max_dn_deg);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+      s->dev.bt_cols = it->second;
+      if (variant) *variant = it->second;
+      if (ms) *ms = -1.0f;
+      return FTLM_OK;
+    }
+  }
+  cudaStream_t st = s->stream;
+  int best_v = 0;
+  float best = 3.4e38f;
+  {
+    std::lock_guard<std::mutex> lock(g_bt_mu);
+    CU_TRY(g_bt.ensure(P.dim, 1));
+    float2* W = g_bt.buf[0].as<float2>();
+    float2* Y = g_bt.buf[1].as<float2>();
+    int* fl = g_bt.flags.as<int>();
+    CU_TRY(bt_start(W, P.dim, 7u, g_bt.st.as<double>(), g_bt.partial.as<double>(), g_bt.used.as<int>(), fl, st,
+                    &s->dev));
+    CU_TRY(cudaMemsetAsync(fl, 0, sizeof(int), st));
+    cudaEvent_t e0, e1;
+    CU_TRY(cudaEventCreate(&e0));
+    CU_TRY(cudaEventCreate(&e1));
+    cudaError_t ce = cudaSuccess;
+    for (int v = 0; v < 3 && ce == cudaSuccess; ++v) {
+      DevSector d = s->dev;
+      d.bt_cols = v;
+      ce = bt_apply(d, W, Y, nullptr, g_bt.partial.as<double>(), fl, st);  // warm-up
+      if (ce == cudaSuccess) ce = cudaEventRecord(e0, st);
+      for (int r = 0; r < reps && ce == cudaSuccess; ++r) ce = bt_apply(d, W, Y, nullptr, g_bt.partial.as<double>(), fl, st);
+      if (ce == cudaSuccess) ce = cudaEventRecord(e1, st);
+      if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+      float t = 0.0f;
+      if (ce == cudaSuccess) ce = cudaEventElapsedTime(&t, e0, e1);
+      if (ce == cudaSuccess && t < best) {
+        best = t;
+        best_v = v;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CU_TRY(ce);
+  }
+  s->dev.bt_cols = best_v;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    cache[key] = best_v;
+  }
+  if (variant) *variant = best_v;
+  if (ms) *ms = best / static_cast<float>(reps);
+  return FTLM_OK;
+}
 
 int ftlm_gpu_batched_lanczos(ftlm_sector* s, int R, int M, unsigned seed, double* alpha, double* beta, int* used) {
   int rc = need_device(s);

@@ -169,16 +169,23 @@ struct ftlm_sector {
     for (void* p : owned) cudaFree(p);
     if (stream) cudaStreamDestroy(stream);
   }
-  int effective_path() const {
-    if (apply_path >= 1 && apply_path <= 3) return (apply_path == 3 && !dev.dn_ent4) ? 2 : apply_path;
-    return ftlm_b200::hv_fast_path_ok(dev_for(2), plan.max_up_deg) ? 2 : 1;
+  // Kernel choice for H·v: 1 = generic gather; 2 = row pass with the per-row coefficient table +
+  // column-slab pass; 3 = row pass in the gauge basis (register-held real coefficients) + column-slab
+  // pass.  Automatic: 3, else 2, else 1.
+  bool path_available(int path) const {
+    if (path == 1) return true;
+    if (path == 3 && !dev.dn_g.ent) return false;
+    return (path == 2 || path == 3) && ftlm_b200::hv_fast_path_ok(dev_for(path), plan.max_up_deg);
   }
-  // The device view a launch of `path` uses: the row pass takes its coefficients from the per-row
-  // shared-memory table (path 2), or from register-held coefficient classes with the compact entry
-  // table (path 3, where the sector has one).
+  int effective_path() const {
+    if (apply_path >= 1 && apply_path <= 3) return (apply_path == 3 && !dev.dn_g.ent) ? 2 : apply_path;
+    if (path_available(3)) return 3;
+    return path_available(2) ? 2 : 1;
+  }
+  // The device view a launch of `path` uses (the row pass reads dn_g on path 3 only).
   ftlm_b200::DevSector dev_for(int path) const {
     ftlm_b200::DevSector d = dev;
-    if (path != 3) d.dn_ent4 = nullptr;
+    if (path != 3) d.dn_g.ent = nullptr;
     return d;
   }
   int apply(const double2* x, double2* y, cudaStream_t st) {

@@ -12,9 +12,9 @@ struct OrbitSectorData {
   DevBuf tlut, tsite, rorder, rank_u, rank_d, rep_full, reta;
   DevBuf uh_from, uh_to, uh_c, uh_own, uh_oth, dh_from, dh_to, dh_c, dh_own, dh_oth;
   int n_uh = 0, n_dh = 0;
-  std::vector<uint32_t> reps_packed;  // all orbit representatives, ascending packed (up<<16 | dn)
-  std::vector<int64_t> reps_full;     // their full-space indices
-  DevBuf reps_dev;                    // reps_packed on the device
+  int64_t nreps = 0;                  // number of orbit representatives of the sector
+  DevBuf reps_dev;                    // [nreps] representatives, ascending packed (up<<16 | dn)
+  DevBuf reps_full_dev;               // [nreps] their full-space indices (int64)
   OrbitDev dev{};
 };
 
@@ -98,23 +98,28 @@ int build_orbit_sector(ftlm_sector* s) {
   CU_TRY(D->rep_full.alloc(static_cast<size_t>(P.dim) * sizeof(int32_t)));
   CU_TRY(D->reta.alloc(static_cast<size_t>(P.dim)));
   CU_TRY(orbit_canon(O, D->rep_full.as<int32_t>(), D->reta.as<uint8_t>(), s->stream));
-  std::vector<int32_t> rf(static_cast<size_t>(P.dim));
-  CU_TRY(cudaMemcpyAsync(rf.data(), D->rep_full.p, rf.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
-  CU_TRY(cudaStreamSynchronize(s->stream));
-  std::vector<std::pair<uint32_t, int64_t>> reps;
-  for (int64_t i = 0; i < P.dim; ++i)
-    if (rf[static_cast<size_t>(i)] == i) {
-      const uint32_t u = P.up.masks[static_cast<size_t>(i / P.dn.D)], d = P.dn.masks[static_cast<size_t>(i % P.dn.D)];
-      reps.emplace_back((u << 16) | d, i);
-    }
-  std::sort(reps.begin(), reps.end());
-  D->reps_packed.resize(reps.size());
-  D->reps_full.resize(reps.size());
-  for (size_t b = 0; b < reps.size(); ++b) {
-    D->reps_packed[b] = reps[b].first;
-    D->reps_full[b] = reps[b].second;
+  {
+    // Representatives in ascending packed order, compacted on the device: position p of that order is
+    // (p / Dd)-th up string by mask value, (p % Dd)-th down string by mask value.
+    std::vector<int32_t> inv_u(static_cast<size_t>(P.up.D)), inv_d(static_cast<size_t>(P.dn.D));
+    for (size_t i = 0; i < inv_u.size(); ++i) inv_u[i] = static_cast<int32_t>(i);
+    for (size_t i = 0; i < inv_d.size(); ++i) inv_d[i] = static_cast<int32_t>(i);
+    std::sort(inv_u.begin(), inv_u.end(),
+              [&P](int32_t a, int32_t b) { return P.up.masks[static_cast<size_t>(a)] < P.up.masks[static_cast<size_t>(b)]; });
+    std::sort(inv_d.begin(), inv_d.end(),
+              [&P](int32_t a, int32_t b) { return P.dn.masks[static_cast<size_t>(a)] < P.dn.masks[static_cast<size_t>(b)]; });
+    DevBuf iu, id, counts;
+    CU_TRY(upload_to(iu, inv_u));
+    CU_TRY(upload_to(id, inv_d));
+    CU_TRY(counts.alloc(static_cast<size_t>(orbit_compact_counts(P.dim)) * sizeof(int32_t)));
+    CU_TRY(orbit_count_reps(O, D->rep_full.as<int32_t>(), iu.as<int32_t>(), id.as<int32_t>(), counts.as<int32_t>(),
+                            &D->nreps, s->stream));
+    CU_TRY(D->reps_dev.alloc(static_cast<size_t>(std::max<int64_t>(D->nreps, 1)) * sizeof(uint32_t)));
+    CU_TRY(D->reps_full_dev.alloc(static_cast<size_t>(std::max<int64_t>(D->nreps, 1)) * sizeof(int64_t)));
+    CU_TRY(orbit_write_reps(O, D->rep_full.as<int32_t>(), iu.as<int32_t>(), id.as<int32_t>(), counts.as<int32_t>(),
+                            D->reps_dev.as<uint32_t>(), D->reps_full_dev.as<int64_t>(), s->stream));
+    CU_TRY(cudaStreamSynchronize(s->stream));
   }
-  CU_TRY(upload_to(D->reps_dev, D->reps_packed));
   // merged hops with their JW masks (same convention as the sector plan)
   std::vector<int32_t> f, t;
   std::vector<double2> c;
@@ -202,42 +207,52 @@ int ftlm_gpu_orbit_create_ex(ftlm_sector* s, int kx, int ky, double survive_tol,
       chi[static_cast<size_t>(dy * s->Lx + dx)] = make_double2(std::cos(theta), std::sin(theta));
     }
   CU_TRY(upload_to(o->chi, chi));
-  const int64_t nreps = static_cast<int64_t>(D.reps_packed.size());
-  DevBuf absA, Adev, sdev;
+  const int64_t nreps = D.nreps;
+  DevBuf absA, Adev, sdev, counts;
   CU_TRY(absA.alloc(std::max<int64_t>(nreps, 1) * sizeof(double)));
   CU_TRY(Adev.alloc(std::max<int64_t>(nreps, 1) * sizeof(double2)));
   CU_TRY(sdev.alloc(std::max<int64_t>(nreps, 1) * sizeof(int)));
+  CU_TRY(counts.alloc(static_cast<size_t>(orbit_compact_counts(nreps)) * sizeof(int32_t)));
   CU_TRY(orbit_absA(D.dev, D.reps_dev.as<uint32_t>(), nreps, o->chi.as<double2>(), absA.as<double>(),
                     Adev.as<double2>(), sdev.as<int>(), s->stream));
-  std::vector<double> aa(static_cast<size_t>(nreps)), AA(static_cast<size_t>(nreps) * 2);
-  std::vector<int> ss(static_cast<size_t>(nreps));
-  CU_TRY(cudaMemcpyAsync(aa.data(), absA.p, aa.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
-  CU_TRY(cudaMemcpyAsync(AA.data(), Adev.p, AA.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
-  CU_TRY(cudaMemcpyAsync(ss.data(), sdev.p, ss.size() * sizeof(int), cudaMemcpyDeviceToHost, s->stream));
-  CU_TRY(cudaStreamSynchronize(s->stream));
-  std::vector<int64_t> full;
-  std::vector<double> sq;
-  for (int64_t b = 0; b < nreps; ++b) {
-    if (aa[static_cast<size_t>(b)] <= survive_tol) continue;  // survive_tol (orbit_k_block_basis.hpp:53)
-    o->reps.push_back(D.reps_packed[static_cast<size_t>(b)]);
-    o->absA.push_back(aa[static_cast<size_t>(b)]);
-    o->Ak.push_back(AA[2 * static_cast<size_t>(b)]);
-    o->Ak.push_back(AA[2 * static_cast<size_t>(b) + 1]);
-    o->stab.push_back(ss[static_cast<size_t>(b)]);
-    o->orbit_idx.push_back(b);
-    full.push_back(D.reps_full[static_cast<size_t>(b)]);
-    sq.push_back(std::sqrt(aa[static_cast<size_t>(b)]));
+  // survivors |A| > survive_tol (orbit_k_block_basis.hpp:53), compacted in order on the device
+  int64_t dk = 0;
+  CU_TRY(orbit_count_survivors(absA.as<double>(), nreps, survive_tol, counts.as<int32_t>(), &dk, s->stream));
+  if (dk >= (1 << 24)) return fail(FTLM_ERR_UNSUPPORTED, "k-block larger than 2^24 states");
+  o->dk = dk;
+  const size_t n1 = static_cast<size_t>(std::max<int64_t>(dk, 1));
+  DevBuf full_k, absA_k, A_k, stab_k, oidx_k;
+  CU_TRY(o->reps_dev.alloc(n1 * sizeof(uint32_t)));
+  CU_TRY(o->sqrtA.alloc(n1 * sizeof(double)));
+  CU_TRY(full_k.alloc(n1 * sizeof(int64_t)));
+  CU_TRY(absA_k.alloc(n1 * sizeof(double)));
+  CU_TRY(A_k.alloc(n1 * sizeof(double2)));
+  CU_TRY(stab_k.alloc(n1 * sizeof(int)));
+  CU_TRY(oidx_k.alloc(n1 * sizeof(int64_t)));
+  const OrbitBlockIn bin{D.reps_dev.as<uint32_t>(), D.reps_full_dev.as<int64_t>(), absA.as<double>(), Adev.as<double2>(),
+                         sdev.as<int>()};
+  const OrbitBlockOut bout{o->reps_dev.as<uint32_t>(), full_k.as<int64_t>(), absA_k.as<double>(), A_k.as<double2>(),
+                           stab_k.as<int>(), oidx_k.as<int64_t>(), o->sqrtA.as<double>()};
+  CU_TRY(orbit_write_survivors(bin, nreps, survive_tol, counts.as<int32_t>(), bout, s->stream));
+  // host copies of the block's entries (ftlm_gpu_orbit_entries / _ex)
+  o->reps.resize(static_cast<size_t>(dk));
+  o->absA.resize(static_cast<size_t>(dk));
+  o->Ak.resize(2 * static_cast<size_t>(dk));
+  o->stab.resize(static_cast<size_t>(dk));
+  o->orbit_idx.resize(static_cast<size_t>(dk));
+  if (dk > 0) {
+    CU_TRY(cudaMemcpyAsync(o->reps.data(), o->reps_dev.p, o->reps.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+    CU_TRY(cudaMemcpyAsync(o->absA.data(), absA_k.p, o->absA.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CU_TRY(cudaMemcpyAsync(o->Ak.data(), A_k.p, o->Ak.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CU_TRY(cudaMemcpyAsync(o->stab.data(), stab_k.p, o->stab.size() * sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CU_TRY(cudaMemcpyAsync(o->orbit_idx.data(), oidx_k.p, o->orbit_idx.size() * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                           s->stream));
   }
-  o->dk = static_cast<int64_t>(o->reps.size());
-  if (o->dk >= (1 << 24)) return fail(FTLM_ERR_UNSUPPORTED, "k-block larger than 2^24 states");
-  CU_TRY(upload_to(o->reps_dev, o->reps));
-  CU_TRY(upload_to(o->sqrtA, sq));
   {
-    DevBuf red, fl;
+    DevBuf red;
     CU_TRY(red.alloc(static_cast<size_t>(s->plan.dim) * sizeof(int32_t)));
     CU_TRY(cudaMemsetAsync(red.p, 0xFF, static_cast<size_t>(s->plan.dim) * sizeof(int32_t), s->stream));
-    CU_TRY(upload_to(fl, full));
-    CU_TRY(orbit_scatter_index(fl.as<int64_t>(), o->dk, red.as<int32_t>(), s->stream));
+    CU_TRY(orbit_scatter_index(full_k.as<int64_t>(), o->dk, red.as<int32_t>(), s->stream));
     CU_TRY(o->table.alloc(static_cast<size_t>(s->plan.dim) * sizeof(uint32_t)));
     CU_TRY(orbit_table(D.dev, D.rep_full.as<int32_t>(), D.reta.as<uint8_t>(), red.as<int32_t>(), o->table.as<uint32_t>(),
                        s->stream));

@@ -6,6 +6,14 @@
 
 namespace ftlm_b200 {
 
+struct DevGauge {
+  const uint32_t* ent;  // entries, [group] rounds of 32
+  const int4* grp;      // [ngroups]: entry offset, real-section rounds, table-section rounds, 0
+  const double2* tab;   // [nt] table-section coefficients
+  int nt;
+  double real2[2];      // real-section coefficients
+};
+
 struct DevSector {
   int n;
   int64_t Du, Dd, dim;
@@ -30,11 +38,10 @@ struct DevSector {
   const uint32_t* dn_nmask;// [n_dn_hops+1]
   int n_dn_hops;           // == pad hop id
   int* flags;              // [0]: input has a non-zero entry with |x|^2 < 1e-28
-  // Compact row-pass table (plan.hpp, SectorPlan::dn_compact); dn_ent4 == nullptr when absent.
-  const uint4* dn_ent4;    // [group][round/4][lane] x 4 entries
-  const int64_t* dn_gptr4; // [ngroups+1], offsets in entries
-  double dn_re[4], dn_im[4];
-  int dn_re_bits, dn_im_bits;  // class-index widths; dn_im_bits < 0: all coefficients real
+  // Gauge-basis down-hop table of the row pass (plan.hpp, GaugeTable); dn_g.ent == nullptr when the
+  // sector has none or the launch uses the per-row table instead.
+  DevGauge dn_g;
+  int bt_cols;              // batched column-pass variant: 0/1/2 = 16/8/4-column chunks
 };
 
 // The reference skips source columns with std::norm(x) < 1e-28

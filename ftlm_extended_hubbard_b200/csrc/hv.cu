@@ -8,9 +8,10 @@
 //   hv_rows     pass 1 of the fast path: persistent CTAs, one output row at a time; the input
 //               row is staged in shared memory (down hops gather inside it); writes
 //               y = diag o x + down part.  Requires a down row (+ coefficient table) to fit in SMEM.
-//               Two forms: hv_rows_compact (coefficient classes in registers, compact 4-entry
-//               loads; the default where the sector's down hops allow it) and hv_rows (per-row
-//               coefficient table in shared memory; any hop list).
+//               Two forms: hv_rows (per-row coefficient table in shared memory; any hop list)
+//               and hv_rows_gauge (the row computed in the spin-ordered basis, where down-hop
+//               coefficients do not depend on the up string: register-held real coefficients,
+//               one shared-memory load per hop; the default where the sector has the table).
 //   hv_cols     pass 2: CTA = (output row, 256-column chunk, two columns per thread), chunk-major so that
 //               the 256-column slab of x stays resident in L2 while all rows read it; adds the
 //               up part: y[r, c] += sum_j coef_j * s_j(c) * x[src_j, c].
@@ -33,6 +34,20 @@ __global__ void __launch_bounds__(256) hv_generic_kernel(DevSector S, const doub
 
 constexpr int kRowThreads = 1024;
 
+// Warm L2 with a row another pass of this CTA reads next (bulk prefetch, no completion to wait on).
+__device__ __forceinline__ void prefetch_row_l2(const double2* row, int64_t n) {
+  const char* p = reinterpret_cast<const char*>(row);
+  const uint32_t bytes = static_cast<uint32_t>(n * static_cast<int64_t>(sizeof(double2)));
+  for (uint32_t off = 0; off < bytes; off += 32768u) {
+    const uint32_t sz = min(32768u, bytes - off);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p + off), "r"(sz) : "memory");
+  }
+}
+
+__device__ __forceinline__ double flip_sign(double v, uint32_t neg) {
+  return __hiloint2double(__double2hiint(v) ^ static_cast<int>(neg << 31), __double2loint(v));
+}
+
 __global__ void __launch_bounds__(kRowThreads, 1) hv_rows_kernel(DevSector S, const double2* __restrict__ x,
                                                                    double2* __restrict__ y, double sx) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -41,15 +56,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) hv_rows_kernel(DevSector S, co
   double2* coef = xs + Dd;
   const int tid = threadIdx.x;
   for (int64_t r = blockIdx.x; r < S.Du; r += gridDim.x) {
-    // Warm L2 with the row this CTA handles next (bulk prefetch, no completion to wait on).
-    if (tid == 0 && r + gridDim.x < S.Du) {
-      const char* nxt = reinterpret_cast<const char*>(x + (r + gridDim.x) * S.Dd);
-      const uint32_t bytes = static_cast<uint32_t>(S.Dd * sizeof(double2));
-      for (uint32_t off = 0; off < bytes; off += 32768u) {
-        const uint32_t sz = min(32768u, bytes - off);
-        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(nxt + off), "r"(sz) : "memory");
-      }
-    }
+    if (tid == 0 && r + gridDim.x < S.Du) prefetch_row_l2(x + (r + gridDim.x) * S.Dd, S.Dd);
     const uint32_t u = S.umask[r];
     const int cuu = S.cnt_uu[r];
     const uint4 w = S.wpl[r];
@@ -96,127 +103,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) hv_rows_kernel(DevSector S, co
   }
 }
 
-// Row pass with the compact down-hop table (SectorPlan::dn_compact): the hop's coefficient comes
-// from a 4-entry class table held in registers (real part, |imaginary part|, sign bit) and its
-// per-row up-string factor from the prefix parity of u, so each hop costs one 16-byte shared load
-// (the x gather) and no coefficient-table load; entries arrive 4 at a time (16-byte loads, two
-// loads ahead).  Same terms in the same order as hv_rows_kernel (the same sums).
-template <int KB>
-__device__ __forceinline__ double pick_class(uint32_t k, const double (&t)[4]) {
-  if constexpr (KB <= 0) {
-    return t[0];
-  } else if constexpr (KB == 1) {
-    return (k & 1u) ? t[1] : t[0];
-  } else {
-    return (k & 2u) ? ((k & 1u) ? t[3] : t[2]) : ((k & 1u) ? t[1] : t[0]);
-  }
-}
-
-__device__ __forceinline__ double flip_sign(double v, uint32_t neg) {
-  return __hiloint2double(__double2hiint(v) ^ static_cast<int>(neg << 31), __double2loint(v));
-}
-
-template <int KR, int KI>
-__device__ __forceinline__ void row_term(double2& acc, uint32_t e, const double2* xs, uint32_t qu,
-                                         const double (&re)[4], const double (&im)[4]) {
-  const double2 v = xs[e & 0x3FFFu];
-  const uint32_t neg = ((qu >> ((e >> 14) & 31u)) ^ (qu >> ((e >> 19) & 31u)) ^ (e >> 24)) & 1u;
-  const double cr = flip_sign(pick_class<KR>((e >> 25) & 3u, re), neg);
-  acc.x = fma(cr, v.x, acc.x);
-  if constexpr (KI >= 0) {
-    const double ci = flip_sign(pick_class<KI>((e >> 27) & 3u, im), neg ^ ((e >> 29) & 1u));
-    acc.x = fma(-ci, v.y, acc.x);
-    acc.y = fma(cr, v.y, acc.y);
-    acc.y = fma(ci, v.x, acc.y);
-  } else {
-    acc.y = fma(cr, v.y, acc.y);
-  }
-}
-
-template <int KR, int KI>
-__global__ void __launch_bounds__(kRowThreads, 1) hv_rows_compact_kernel(DevSector S, const double2* __restrict__ x,
-                                                                           double2* __restrict__ y, double sx) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int Dd = static_cast<int>(S.Dd);
-  double2* xs = reinterpret_cast<double2*>(smem_raw);
-  const int tid = threadIdx.x;
-  double re[4], im[4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    re[i] = S.dn_re[i];
-    im[i] = S.dn_im[i];
-  }
-  if (tid < 8) xs[Dd + tid] = make_double2(0.0, 0.0);  // zero sentinels for padding entries
-  for (int64_t r = blockIdx.x; r < S.Du; r += gridDim.x) {
-    if (tid == 0 && r + gridDim.x < S.Du) {
-      const char* nxt = reinterpret_cast<const char*>(x + (r + gridDim.x) * S.Dd);
-      const uint32_t bytes = static_cast<uint32_t>(S.Dd * sizeof(double2));
-      for (uint32_t off = 0; off < bytes; off += 32768u) {
-        const uint32_t sz = min(32768u, bytes - off);
-        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(nxt + off), "r"(sz) : "memory");
-      }
-    }
-    const uint32_t u = S.umask[r];
-    const uint32_t qu = prefix_parity_shifted(u);
-    const int cuu = S.cnt_uu[r];
-    const uint4 w = S.wpl[r];
-    const double2* xrow = x + r * S.Dd;
-    int saw_tiny = 0;
-    for (int c = tid; c < Dd; c += kRowThreads) {
-      double2 v = xrow[c];
-      v.x *= sx;
-      v.y *= sx;
-      if (tiny(v)) {
-        saw_tiny |= (v.x != 0.0 || v.y != 0.0);
-        v = make_double2(0.0, 0.0);
-      }
-      xs[c] = v;
-    }
-    if (saw_tiny) atomicOr(S.flags, 1);
-    __syncthreads();
-    double2* yrow = y + r * S.Dd;
-    for (int c = tid; c < Dd; c += kRowThreads) {
-      const double2 xv = xs[c];
-      const double dg = diag_value(S, u, S.dmask[c], cuu, S.cnt_dd[c], w);
-      double2 acc = make_double2(dg * xv.x, dg * xv.y);
-      const int g = c >> 5;
-      const int64_t b0 = S.dn_gptr4[g];
-      const int nq = static_cast<int>((S.dn_gptr4[g + 1] - b0) >> 7);  // 16-byte loads per lane
-      const uint4* ep = S.dn_ent4 + (b0 >> 2) + (c & 31);
-      uint4 cur = __ldg(ep);
-      uint4 nxt = nq > 1 ? __ldg(ep + 32) : cur;
-      for (int q = 0; q < nq; ++q) {
-        const uint4 e = cur;
-        cur = nxt;
-        if (q + 2 < nq) nxt = __ldg(ep + (q + 2) * 32);
-        row_term<KR, KI>(acc, e.x, xs, qu, re, im);
-        row_term<KR, KI>(acc, e.y, xs, qu, re, im);
-        row_term<KR, KI>(acc, e.z, xs, qu, re, im);
-        row_term<KR, KI>(acc, e.w, xs, qu, re, im);
-      }
-      yrow[c] = acc;
-    }
-    __syncthreads();
-  }
-}
-
 using RowsKernel = void (*)(DevSector, const double2*, double2*, double);
-
-template <int KR>
-RowsKernel rows_compact_for(int ki) {
-  switch (ki) {
-    case -1: return hv_rows_compact_kernel<KR, -1>;
-    case 0: return hv_rows_compact_kernel<KR, 0>;
-    case 1: return hv_rows_compact_kernel<KR, 1>;
-    default: return hv_rows_compact_kernel<KR, 2>;
-  }
-}
-
-RowsKernel rows_compact(int kr, int ki) {
-  if (kr <= 0) return rows_compact_for<0>(ki);
-  if (kr == 1) return rows_compact_for<1>(ki);
-  return rows_compact_for<2>(ki);
-}
 
 // Column pass: two columns per thread, chunk = 2 * threads columns (variants: 64 / 128 / 256
 // threads = 128 / 256 / 512-column slabs of Du * chunk * 16 bytes kept in L2; the autotuner picks).
@@ -231,6 +118,103 @@ __device__ __forceinline__ void cmac_xor(double2& acc, double2 c, double2 v, uin
   acc.x = fma(-c.y, v.y, acc.x);
   acc.y = fma(c.x, v.y, acc.y);
   acc.y = fma(c.y, v.x, acc.y);
+}
+
+// One entry of a gauge table: the real section takes its coefficient from two registers, the table
+// section from the 8-copy table (copy i % 8: the 8 lanes of a quarter-warp hit 8 bank groups).
+__device__ __forceinline__ void gauge_term(double2& acc, uint32_t e, bool real, int i, const unsigned char* line,
+                                           const double2* tab, double a0, double a1) {
+  const double2 v = *reinterpret_cast<const double2*>(line + (e & 0x3FFF0u));
+  if (real) {
+    const double cf = flip_sign((e & 0x40000000u) ? a1 : a0, e >> 31);
+    acc.x = fma(cf, v.x, acc.x);
+    acc.y = fma(cf, v.y, acc.y);
+  } else {
+    cmac_xor(acc, tab[((e >> 18) & 511u) * 8 + (i & 7)], v, e >> 31);
+  }
+}
+
+// acc += sum over the gauge-table entries of output string i (one warp = 32 consecutive strings, so
+// the round counts are warp-uniform): 4 rounds per 16-byte load, two loads ahead of their use.
+__device__ __forceinline__ void gauge_hops(double2& acc, const DevGauge& G, int i, const unsigned char* line,
+                                           const double2* tab, double a0, double a1) {
+  const int4 gp = G.grp[i >> 5];
+  const int kr = gp.y, kt = kr + gp.z;
+  const int nq = (kt + 3) >> 2;
+  const uint4* ep = reinterpret_cast<const uint4*>(G.ent + gp.x) + (i & 31);
+  uint4 cur = nq > 0 ? __ldg(ep) : make_uint4(0u, 0u, 0u, 0u);
+  uint4 nxt = nq > 1 ? __ldg(ep + 32) : cur;
+  for (int q = 0; q < nq; ++q) {
+    const uint4 e = cur;
+    cur = nxt;
+    if (q + 2 < nq) nxt = __ldg(ep + (q + 2) * 32);
+    const int k = 4 * q;
+    if (k + 3 < kr) {  // all four in the real section (the common case)
+      gauge_term(acc, e.x, true, i, line, tab, a0, a1);
+      gauge_term(acc, e.y, true, i, line, tab, a0, a1);
+      gauge_term(acc, e.z, true, i, line, tab, a0, a1);
+      gauge_term(acc, e.w, true, i, line, tab, a0, a1);
+    } else {
+      if (k < kt) gauge_term(acc, e.x, k < kr, i, line, tab, a0, a1);
+      if (k + 1 < kt) gauge_term(acc, e.y, k + 1 < kr, i, line, tab, a0, a1);
+      if (k + 2 < kt) gauge_term(acc, e.z, k + 2 < kr, i, line, tab, a0, a1);
+      if (k + 3 < kt) gauge_term(acc, e.w, k + 3 < kr, i, line, tab, a0, a1);
+    }
+  }
+}
+
+// Row pass in the spin-ordered basis.  With g(u, d) = (-1)^popc(u & prefix_parity_shifted(d)), the
+// down-hop part of row u is  y[u, d] = g(u, d) sum_h (-1)^s_h c_h g(u, d_h) x[u, d_h]  with s_h the
+// down-string sign alone, so the row is staged as xs[d] = g(u, d) x[u, d] and every coefficient is
+// the same for all rows: real ones come from two registers (an entry bit picks one), the others from
+// a small table copied once per CTA (8 copies, one per bank group).  Each hop then costs one 16-byte
+// shared load of x (plus one for table hops) instead of two.  Entries: GaugeTable (plan.hpp).
+__global__ void __launch_bounds__(kRowThreads, 1) hv_rows_gauge_kernel(DevSector S, const double2* __restrict__ x,
+                                                                         double2* __restrict__ y, double sx) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int Dd = static_cast<int>(S.Dd);
+  double2* xs = reinterpret_cast<double2*>(smem_raw);
+  double2* tab = xs + Dd + 8;
+  const int tid = threadIdx.x;
+  const DevGauge G = S.dn_g;
+  for (int i = tid; i < G.nt * 8; i += kRowThreads) tab[i] = G.tab[i >> 3];
+  if (tid < 8) xs[Dd + tid] = make_double2(0.0, 0.0);  // zero sentinels for padding entries
+  const double a0 = G.real2[0], a1 = G.real2[1];
+  for (int64_t r = blockIdx.x; r < S.Du; r += gridDim.x) {
+    if (tid == 0 && r + gridDim.x < S.Du) prefetch_row_l2(x + (r + gridDim.x) * S.Dd, S.Dd);
+    const uint32_t u = S.umask[r];
+    const int cuu = S.cnt_uu[r];
+    const uint4 w = S.wpl[r];
+    const double2* xrow = x + r * S.Dd;
+    uint32_t gbits = 0;  // bit j: g(u, d) of this thread's element j (d = tid + j * kRowThreads)
+    int saw_tiny = 0;
+    for (int c = tid, j = 0; c < Dd; c += kRowThreads, ++j) {
+      double2 v = xrow[c];
+      v.x *= sx;  // the input is sx * x (sx = 1: unchanged)
+      v.y *= sx;
+      if (tiny(v)) {
+        saw_tiny |= (v.x != 0.0 || v.y != 0.0);
+        v = make_double2(0.0, 0.0);
+      }
+      if (gauge_sign(u, S.dmask[c])) {
+        v = make_double2(-v.x, -v.y);
+        gbits |= 1u << j;
+      }
+      xs[c] = v;
+    }
+    if (saw_tiny) atomicOr(S.flags, 1);
+    __syncthreads();
+    double2* yrow = y + r * S.Dd;
+    for (int c = tid, j = 0; c < Dd; c += kRowThreads, ++j) {
+      const double2 xv = xs[c];
+      const double dg = diag_value(S, u, S.dmask[c], cuu, S.cnt_dd[c], w);
+      double2 acc = make_double2(dg * xv.x, dg * xv.y);
+      gauge_hops(acc, G, c, smem_raw, tab, a0, a1);
+      if ((gbits >> j) & 1u) acc = make_double2(-acc.x, -acc.y);
+      yrow[c] = acc;
+    }
+    __syncthreads();
+  }
 }
 
 // kFused: the input is sx * x; the up-hop sum is formed on its own and added as
@@ -350,7 +334,7 @@ int g_num_sms = 0;
 }  // namespace
 
 size_t hv_rows_smem_bytes(const DevSector& S) {
-  if (S.dn_ent4) return static_cast<size_t>(S.Dd + 8) * sizeof(double2);
+  if (S.dn_g.ent) return static_cast<size_t>(S.Dd + 8 + 8 * S.dn_g.nt) * sizeof(double2);
   return static_cast<size_t>(S.Dd) * sizeof(double2) + static_cast<size_t>(S.n_dn_hops + 1) * 8 * sizeof(double2);
 }
 
@@ -391,7 +375,7 @@ cudaError_t hv_launch_pass(const DevSector& S, const double2* x, double2* y, int
     cudaError_t e = cudaMemsetAsync(S.flags, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
     const size_t sm = hv_rows_smem_bytes(S);
-    const RowsKernel k = S.dn_ent4 ? rows_compact(S.dn_re_bits, S.dn_im_bits) : hv_rows_kernel;
+    const RowsKernel k = S.dn_g.ent ? hv_rows_gauge_kernel : hv_rows_kernel;
     e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
     if (e != cudaSuccess) return e;
     const int grid_r = static_cast<int>(std::min<int64_t>(S.Du, g_num_sms));

@@ -7,7 +7,8 @@
 
 namespace ftlm_b200 {
 
-// path: 1 = generic gather kernel, 2 = row pass + column-slab pass.  cols_variant: column slab of
+// path: 1 = generic gather kernel, 2 = row pass + column-slab pass.  The row pass reads the gauge
+// table when S.dn_g.ent is set (else the per-row coefficient table).  cols_variant: column slab of
 // 256 (0), 128 (1) or 512 (2) columns.
 cudaError_t hv_launch(const DevSector& S, const double2* x, double2* y, int path, cudaStream_t st,
                       int cols_variant = 0);

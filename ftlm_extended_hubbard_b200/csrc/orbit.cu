@@ -257,6 +257,162 @@ __global__ void scatter_kernel(const int64_t* __restrict__ full, int64_t n, int3
 }
 
 int g_sms = 0;
+// Order-preserving stream compaction: kCompactItems consecutive items per block (4 per thread, in
+// thread order), block counts, one-block exclusive scan of the counts, then each block writes its
+// flagged items at offset + in-block prefix.  Pred(p) -> bool, Emit(p, pos).
+constexpr int kCompactThreads = 1024;
+constexpr int kCompactItems = 4 * kCompactThreads;
+
+template <class Pred>
+__global__ void __launch_bounds__(kCompactThreads) compact_count_kernel(Pred pred, int64_t n, int32_t* counts) {
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * kCompactItems + 4 * threadIdx.x;
+  int c = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) c += (base + k < n && pred(base + k)) ? 1 : 0;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  __shared__ int ws[kCompactThreads / 32];
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < kCompactThreads / 32; ++w) t += ws[w];
+    counts[blockIdx.x] = t;
+  }
+}
+
+// counts[0..nb) -> exclusive offsets in place, total in counts[nb] (one block, chunks of 1024).
+__global__ void __launch_bounds__(kCompactThreads) compact_scan_kernel(int32_t* counts, int64_t nb) {
+  __shared__ int32_t buf[kCompactThreads];
+  __shared__ int32_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int64_t b0 = 0; b0 < nb; b0 += kCompactThreads) {
+    const int64_t b = b0 + threadIdx.x;
+    const int32_t v = b < nb ? counts[b] : 0;
+    buf[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = 1; o < kCompactThreads; o <<= 1) {  // Hillis-Steele inclusive scan
+      const int32_t add = threadIdx.x >= static_cast<unsigned>(o) ? buf[threadIdx.x - o] : 0;
+      __syncthreads();
+      buf[threadIdx.x] += add;
+      __syncthreads();
+    }
+    if (b < nb) counts[b] = carry + buf[threadIdx.x] - v;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += buf[kCompactThreads - 1];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) counts[nb] = carry;
+}
+
+template <class Pred, class Emit>
+__global__ void __launch_bounds__(kCompactThreads) compact_write_kernel(Pred pred, Emit emit, int64_t n,
+                                                                         const int32_t* offsets) {
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * kCompactItems + 4 * threadIdx.x;
+  bool f[4];
+  int c = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    f[k] = base + k < n && pred(base + k);
+    c += f[k] ? 1 : 0;
+  }
+  // exclusive prefix of c over the block (thread order)
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int incl = c;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  __shared__ int ws[kCompactThreads / 32];
+  if (lane == 31) ws[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    int v = ws[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += u;
+    }
+    ws[lane] = v;
+  }
+  __syncthreads();
+  int pos = offsets[blockIdx.x] + (warp > 0 ? ws[warp - 1] : 0) + incl - c;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (f[k]) emit(base + k, pos++);
+}
+
+// Phase 1: per-block counts, their exclusive scan and the total (synchronises st to read it back).
+template <class Pred>
+cudaError_t compact_count(Pred pred, int64_t n, int32_t* counts /* >= nb + 1 */, int64_t* total, cudaStream_t st) {
+  *total = 0;
+  if (n <= 0) return cudaSuccess;
+  const int64_t nb = (n + kCompactItems - 1) / kCompactItems;
+  compact_count_kernel<<<static_cast<unsigned>(nb), kCompactThreads, 0, st>>>(pred, n, counts);
+  compact_scan_kernel<<<1, kCompactThreads, 0, st>>>(counts, nb);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  int32_t t = 0;
+  e = cudaMemcpyAsync(&t, counts + nb, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  *total = t;
+  return e;
+}
+
+// Phase 2: the flagged items, in order, to the outputs sized by phase 1.
+template <class Pred, class Emit>
+cudaError_t compact_write(Pred pred, Emit emit, int64_t n, const int32_t* counts, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int64_t nb = (n + kCompactItems - 1) / kCompactItems;
+  compact_write_kernel<<<static_cast<unsigned>(nb), kCompactThreads, 0, st>>>(pred, emit, n, counts);
+  return cudaGetLastError();
+}
+
+// Position p of the packed order (up strings by mask value, then down strings by mask value) is the
+// full state inv_u[p / Dd] * Dd + inv_d[p % Dd]; it is listed when it is its orbit's representative.
+struct RepPred {
+  const int32_t* rep_full;
+  const int32_t* inv_u;
+  const int32_t* inv_d;
+  int64_t Dd;
+  __device__ bool operator()(int64_t p) const {
+    const int64_t i = static_cast<int64_t>(inv_u[p / Dd]) * Dd + inv_d[p % Dd];
+    return rep_full[i] == i;
+  }
+};
+struct RepEmit {
+  const int32_t* inv_u;
+  const int32_t* inv_d;
+  const uint32_t* umask;
+  const uint32_t* dmask;
+  int64_t Dd;
+  uint32_t* packed;
+  int64_t* full;
+  __device__ void operator()(int64_t p, int pos) const {
+    const int32_t ru = inv_u[p / Dd], rd = inv_d[p % Dd];
+    packed[pos] = (umask[ru] << 16) | dmask[rd];
+    full[pos] = static_cast<int64_t>(ru) * Dd + rd;
+  }
+};
+
+struct SurvivePred {
+  const double* absA;
+  double tol;
+  __device__ bool operator()(int64_t b) const { return absA[b] > tol; }
+};
+struct SurviveEmit {
+  OrbitBlockIn in;
+  OrbitBlockOut out;
+  __device__ void operator()(int64_t b, int pos) const {
+    out.reps[pos] = in.reps[b];
+    out.absA[pos] = in.absA[b];
+    out.A[pos] = in.A[b];
+    out.stab[pos] = in.stab[b];
+    out.orbit_idx[pos] = b;
+    out.full[pos] = in.full[b];
+    out.sqrtA[pos] = sqrt(in.absA[b]);
+  }
+};
+
 unsigned grid_for(int64_t n) {
   if (g_sms == 0) {
     int dev = 0;
@@ -269,6 +425,29 @@ unsigned grid_for(int64_t n) {
 }
 
 }  // namespace
+
+int64_t orbit_compact_counts(int64_t n) { return (n + kCompactItems - 1) / kCompactItems + 1; }
+
+cudaError_t orbit_count_reps(const OrbitDev& O, const int32_t* rep_full, const int32_t* inv_u, const int32_t* inv_d,
+                             int32_t* counts, int64_t* nreps, cudaStream_t st) {
+  return compact_count(RepPred{rep_full, inv_u, inv_d, O.Dd}, O.dim, counts, nreps, st);
+}
+
+cudaError_t orbit_write_reps(const OrbitDev& O, const int32_t* rep_full, const int32_t* inv_u, const int32_t* inv_d,
+                             const int32_t* counts, uint32_t* packed, int64_t* full, cudaStream_t st) {
+  return compact_write(RepPred{rep_full, inv_u, inv_d, O.Dd},
+                       RepEmit{inv_u, inv_d, O.umask, O.dmask, O.Dd, packed, full}, O.dim, counts, st);
+}
+
+cudaError_t orbit_count_survivors(const double* absA, int64_t nreps, double tol, int32_t* counts, int64_t* dk,
+                                  cudaStream_t st) {
+  return compact_count(SurvivePred{absA, tol}, nreps, counts, dk, st);
+}
+
+cudaError_t orbit_write_survivors(const OrbitBlockIn& in, int64_t nreps, double tol, const int32_t* counts,
+                                  const OrbitBlockOut& out, cudaStream_t st) {
+  return compact_write(SurvivePred{in.absA, tol}, SurviveEmit{in, out}, nreps, counts, st);
+}
 
 cudaError_t orbit_canon(const OrbitDev& O, int32_t* rep_full, uint8_t* reta, cudaStream_t st) {
   canon_kernel<<<grid_for(O.dim), 256, 0, st>>>(O, rep_full, reta);

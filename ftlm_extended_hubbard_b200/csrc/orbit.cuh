@@ -26,6 +26,39 @@ struct OrbitDev {
 // Per full state: full index of its canonical representative, and (R | eta<<4) with
 // T_R rep = state (first R in the reference's search order), eta = fermionic sign of T_R on rep.
 cudaError_t orbit_canon(const OrbitDev& O, int32_t* rep_full, uint8_t* reta, cudaStream_t st);
+// Order-preserving device compaction (scratch `counts` of orbit_compact_counts(n) ints): a count
+// call (synchronises st to return the number) and a write call into outputs of that size.
+int64_t orbit_compact_counts(int64_t n);
+// The sector's orbit representatives in ascending packed (up<<16 | dn) order: inv_u / inv_d list the
+// up / down ranks by ascending mask value; packed[], full[] receive the representatives and their
+// full indices.
+cudaError_t orbit_count_reps(const OrbitDev& O, const int32_t* rep_full, const int32_t* inv_u, const int32_t* inv_d,
+                             int32_t* counts, int64_t* nreps, cudaStream_t st);
+cudaError_t orbit_write_reps(const OrbitDev& O, const int32_t* rep_full, const int32_t* inv_u, const int32_t* inv_d,
+                             const int32_t* counts, uint32_t* packed, int64_t* full, cudaStream_t st);
+
+// The representatives of one momentum block: those with |A(K)| > tol, in order.
+struct OrbitBlockIn {
+  const uint32_t* reps;   // [nreps] packed, ascending
+  const int64_t* full;    // [nreps]
+  const double* absA;     // [nreps]
+  const double2* A;       // [nreps]
+  const int* stab;        // [nreps]
+};
+struct OrbitBlockOut {
+  uint32_t* reps;
+  int64_t* full;
+  double* absA;
+  double2* A;
+  int* stab;
+  int64_t* orbit_idx;     // index among all representatives
+  double* sqrtA;
+};
+cudaError_t orbit_count_survivors(const double* absA, int64_t nreps, double tol, int32_t* counts, int64_t* dk,
+                                  cudaStream_t st);
+cudaError_t orbit_write_survivors(const OrbitBlockIn& in, int64_t nreps, double tol, const int32_t* counts,
+                                  const OrbitBlockOut& out, cudaStream_t st);
+
 // |A(K)| per representative: A = sum over stabiliser S of eta(rep,S) chi*(S) (chi* from chi_tab);
 // optionally A itself and the stabiliser size (A, stab may be null).
 cudaError_t orbit_absA(const OrbitDev& O, const uint32_t* reps_packed, int64_t nreps, const double2* chi_tab,

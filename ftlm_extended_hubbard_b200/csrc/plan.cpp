@@ -2,6 +2,7 @@
 #include "plan.hpp"
 
 #include <algorithm>
+#include <cstdint>
 #include <cmath>
 #include <complex>
 #include <map>
@@ -151,69 +152,101 @@ void schedule_quarter(const std::vector<uint32_t>* in, std::vector<uint32_t>* ou
   }
 }
 
-// Index of v in the class list (appended when new and there is room), or -1.
-int class_of(double v, double* list, int* n) {
-  for (int i = 0; i < *n; ++i)
-    if (list[i] == v) return i;
-  if (*n >= 4) return -1;
-  list[*n] = v;
-  return (*n)++;
-}
-
-int bits_for(int n) { return n <= 1 ? 0 : (n <= 2 ? 1 : 2); }
-
-// The compact row-pass table (see SectorPlan::dn_compact): the entries of dn_ent re-encoded with
-// the hop's sites and coefficient classes instead of its id.
-void build_compact_down(SectorPlan* Pp) {
-  SectorPlan& P = *Pp;
-  P.dn_compact = false;
-  P.dn_gptr4.clear();
-  P.dn_ent4.clear();
-  const int64_t Dd = P.dn.D;
-  if (P.n > 31 || Dd + 8 > (1 << 14) || P.dn_gptr.size() < 2) return;
-  const int nh = static_cast<int>(P.hd.size());
-  std::vector<uint32_t> code(static_cast<size_t>(nh) + 1, 0u);
-  int nre = 0, nim = 0;
+// The gauge-basis gather table of one spin (see GaugeTable): per group of 32 output strings, the
+// hops split into the real section (coefficient one of two register-held values) and the table
+// section, each scheduled by schedule_quarter, then re-encoded with byte offsets and sentinels.
+void build_gauge_table(const SpinSpace& sp, const std::vector<MergedHop>& hops, int n_sites, GaugeTable* out) {
+  GaugeTable& G = *out;
+  G = GaugeTable{};
+  const int64_t D = sp.D;
+  if (n_sites > 32 || D < 1 || D + 8 > (1 << 14)) return;
+  const int nh = static_cast<int>(hops.size());
+  if (nh >= 511) return;
+  // class of each hop: 0/1 = real value real2[0/1], 2 + t = table entry t
+  std::vector<int> cls(static_cast<size_t>(nh), 0);
+  int nreal = 0;
   for (int h = 0; h < nh; ++h) {
-    const MergedHop& m = P.hd[static_cast<size_t>(h)];
-    const int kr = class_of(m.cre, P.dn_re, &nre);
-    const int ki = class_of(std::fabs(m.cim), P.dn_im, &nim);
-    if (kr < 0 || ki < 0) return;
-    code[static_cast<size_t>(h)] = (static_cast<uint32_t>(m.lo + 1) << 14) | (static_cast<uint32_t>(m.hi + 1) << 19) |
-                                   (static_cast<uint32_t>(kr) << 25) | (static_cast<uint32_t>(ki) << 27) |
-                                   (static_cast<uint32_t>(std::signbit(m.cim) ? 1 : 0) << 29);
-  }
-  P.dn_re_bits = bits_for(nre);
-  P.dn_im_bits = (nim <= 1 && P.dn_im[0] == 0.0) ? -1 : bits_for(nim);
-  auto sentinel = [Dd](uint32_t group) {
-    return static_cast<uint32_t>(Dd + static_cast<int64_t>((group + 8 - static_cast<uint32_t>(Dd & 7)) & 7));
-  };
-  const int64_t ngroups = static_cast<int64_t>(P.dn_gptr.size()) - 1;
-  P.dn_gptr4.assign(static_cast<size_t>(ngroups) + 1, 0);
-  for (int64_t g = 0; g < ngroups; ++g) {
-    const int64_t base = P.dn_gptr[static_cast<size_t>(g)];
-    const int64_t K = (P.dn_gptr[static_cast<size_t>(g) + 1] - base) / 32;
-    const int64_t K4 = (K + 3) / 4 * 4;
-    const size_t off = P.dn_ent4.size();
-    P.dn_ent4.resize(off + static_cast<size_t>(K4) * 32, 0u);
-    for (int64_t k = 0; k < K4; ++k)
-      for (uint32_t l = 0; l < 32; ++l) {
-        uint32_t out;
-        if (k < K) {
-          const uint32_t e = P.dn_ent[static_cast<size_t>(base + 32 * k + l)];
-          const uint32_t src = e >> 10, h = (e >> 1) & 511u;
-          if (static_cast<int>(h) == P.dn_pad_hop)
-            out = sentinel(src & 7u);  // zero element in the same bank group: zero contribution
-          else
-            out = src | code[h] | ((e & 1u) << 24);
-        } else {
-          out = sentinel(l & 7u);  // extra rounds: the 8 lanes of a quarter hit 8 distinct groups
-        }
-        P.dn_ent4[off + static_cast<size_t>(((k / 4) * 32 + l) * 4 + (k % 4))] = out;
+    const MergedHop& m = hops[static_cast<size_t>(h)];
+    int k = -1;
+    if (m.cim == 0.0) {
+      for (int i = 0; i < nreal; ++i)
+        if (G.real2[i] == m.cre) k = i;
+      if (k < 0 && nreal < 2) {
+        G.real2[nreal] = m.cre;
+        k = nreal++;
       }
-    P.dn_gptr4[static_cast<size_t>(g) + 1] = static_cast<int64_t>(P.dn_ent4.size());
+    }
+    if (k < 0) {
+      k = 2 + static_cast<int>(G.tab.size() / 2);
+      G.tab.push_back(m.cre);
+      G.tab.push_back(m.cim);
+    }
+    cls[static_cast<size_t>(h)] = k;
   }
-  P.dn_compact = true;
+  if (nreal == 1) G.real2[1] = G.real2[0];
+  if (G.tab.size() / 2 > 512) return;
+  auto sentinel = [D](uint32_t group) {
+    return static_cast<uint32_t>(D + static_cast<int64_t>((group + 8u - static_cast<uint32_t>(D & 7)) & 7u)) << 4;
+  };
+  const uint32_t pad_hop = static_cast<uint32_t>(nh) << 1;
+  // old-format entry (src<<10 | hop<<1 | s) -> section entry; pads become sentinels of their bank group
+  auto encode = [&](uint32_t e) -> uint32_t {
+    const uint32_t src = e >> 10, h = (e >> 1) & 511u, sg = e & 1u;
+    if (static_cast<int>(h) == nh) return sentinel(src & 7u);
+    const int k = cls[h];
+    if (k < 2) return (src << 4) | (static_cast<uint32_t>(k) << 30) | (sg << 31);
+    return (src << 4) | (static_cast<uint32_t>(k - 2) << 18) | (sg << 31);
+  };
+  const int64_t ngroups = (D + 31) / 32;
+  std::vector<std::vector<uint32_t>> lr(32), lt(32), sr(32), st(32);
+  for (int64_t g = 0; g < ngroups; ++g) {
+    for (int l = 0; l < 32; ++l) {
+      lr[l].clear();
+      lt[l].clear();
+      const int64_t r = g * 32 + l;
+      if (r >= D) continue;
+      const uint32_t m2 = sp.masks[static_cast<size_t>(r)];
+      for (int h = 0; h < nh; ++h) {
+        const auto& hp = hops[static_cast<size_t>(h)];
+        if (!((m2 >> hp.to) & 1u) || ((m2 >> hp.from) & 1u)) continue;
+        const uint32_t m = m2 ^ (1u << hp.from) ^ (1u << hp.to);
+        const int64_t src = sp.rank(m);
+        if (src < 0) return;
+        const uint32_t sg = static_cast<uint32_t>(popc(m & hp.own_mask) & 1);
+        const uint32_t e = (static_cast<uint32_t>(src) << 10) | (static_cast<uint32_t>(h) << 1) | sg;
+        (cls[static_cast<size_t>(h)] < 2 ? lr[l] : lt[l]).push_back(e);
+      }
+    }
+    size_t KR = 0, KT = 0;
+    for (int qw = 0; qw < 4; ++qw) {
+      schedule_quarter(&lr[8 * qw], &sr[8 * qw], pad_hop, D);
+      schedule_quarter(&lt[8 * qw], &st[8 * qw], pad_hop, D);
+      KR = std::max(KR, sr[8 * qw].size());
+      KT = std::max(KT, st[8 * qw].size());
+    }
+    const size_t K4 = (KR + KT + 3) / 4 * 4;
+    const size_t off = G.ent.size();
+    if (off + K4 * 32 > static_cast<size_t>(INT32_MAX)) return;
+    G.grp.push_back(static_cast<int32_t>(off));
+    G.grp.push_back(static_cast<int32_t>(KR));
+    G.grp.push_back(static_cast<int32_t>(KT));
+    G.grp.push_back(0);
+    // round k of lane l at off + ((k / 4) * 32 + l) * 4 + k % 4: a lane loads 4 rounds with one
+    // 16-byte load.  Rounds a quarter does not need, and the rounds that pad the group to a
+    // multiple of 4: lane l reads the sentinel of bank group l % 8.
+    G.ent.resize(off + K4 * 32);
+    for (size_t k = 0; k < K4; ++k)
+      for (int l = 0; l < 32; ++l) {
+        uint32_t e = sentinel(static_cast<uint32_t>(l) & 7u);
+        if (k < KR) {
+          if (k < sr[l].size()) e = encode(sr[l][k]);
+        } else if (k < KR + KT) {
+          if (k - KR < st[l].size()) e = encode(st[l][k - KR]);
+        }
+        G.ent[off + ((k / 4) * 32 + static_cast<size_t>(l)) * 4 + k % 4] = e;
+      }
+  }
+  G.ok = true;
 }
 
 }  // namespace
@@ -462,7 +495,7 @@ std::string build_plan(int n_sites, int n_up, int n_dn, double U, double V, cons
     P.dn_gptr[static_cast<size_t>(g) + 1] = static_cast<int64_t>(P.dn_ent.size());
   }
   P.mean_dn_sources = P.dn.D ? static_cast<double>(total_src) / static_cast<double>(P.dn.D) : 0.0;
-  build_compact_down(&P);
+  build_gauge_table(P.dn, P.hd, P.n, &P.dn_g);
   return "";
 }
 

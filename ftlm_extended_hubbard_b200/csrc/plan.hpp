@@ -50,6 +50,28 @@ struct MergedHop {
   int lo, hi;
 };
 
+// Hop gather table of one spin in the spin-ordered (gauge) basis g(u, d) = (-1)^popc(u & pps(d)),
+// pps(d) = prefix parity of d shifted by one site.  In that basis a hop's coefficient is (-1)^s c_h,
+// s the JW sign of the hopping species' own string alone, so the same table serves every string of
+// the other species.  Built when D + 8 <= 16384, n_sites <= 32 and at most 512 hops need a table
+// coefficient.  Per group of 32 output strings, rounds k = 0 .. KR+KT-1 (padded to a multiple of 4),
+// entry of round k for lane l at grp[4g] + ((k / 4) * 32 + l) * 4 + k % 4 (one 16-byte load per
+// lane brings 4 rounds):
+//   real section  (rounds k < KR = grp[4g+1]): hops with c_h = real2[cls], cls in {0, 1};
+//                 entry = src<<4 | cls<<30 | s<<31
+//   table section (KR <= k < KR + KT, KT = grp[4g+2]): any other hop; entry = src<<4 | t<<18 | s<<31
+//                 with c_h = (tab[2t], tab[2t+1])
+// src << 4 is the byte offset of the 16-byte element in the staged line; src >= D addresses one of 8
+// zero sentinels after it (padding, one per bank group).  Each section is scheduled so that the 8
+// lanes of a quarter-warp read 8 different bank groups in every round.
+struct GaugeTable {
+  bool ok = false;
+  double real2[2] = {0.0, 0.0};
+  std::vector<double> tab;
+  std::vector<int32_t> grp;
+  std::vector<uint32_t> ent;
+};
+
 struct SectorPlan {
   int n = 0, nu = 0, nd = 0;
   double U = 0.0, V = 0.0;
@@ -82,18 +104,8 @@ struct SectorPlan {
   std::vector<double> dn_coef;     // 2 per hop id (pad hop id has 0)
   std::vector<uint32_t> dn_nmask;  // per hop id
 
-  // Compact row-pass table (same entries and order as dn_ent), built when the merged down-hop
-  // coefficients take at most 4 distinct real parts and 4 distinct |imaginary parts|,
-  // Dd + 8 <= 16384 and n_sites <= 31.  Entry = src | (lo+1)<<14 | (hi+1)<<19 | dn_sign<<24 |
-  // re_class<<25 | im_class<<27 | im_negative<<29; the per-row up-string factor is
-  // parity(u in (lo, hi]) from the up string's prefix parity; src >= Dd addresses one of 8 zero
-  // sentinels after the staged row (padding, one per bank group).  Rounds are padded to a multiple
-  // of 4 and stored [group][round/4][lane][4] so that a lane loads 4 entries with one 16-byte load.
-  bool dn_compact = false;
-  int dn_re_bits = 0, dn_im_bits = 0;  // class-index widths (0, 1 or 2); dn_im_bits = -1: all real
-  double dn_re[4] = {0, 0, 0, 0}, dn_im[4] = {0, 0, 0, 0};
-  std::vector<int64_t> dn_gptr4;  // per group, offset in entries (multiple of 128)
-  std::vector<uint32_t> dn_ent4;
+  // Down-hop gather table of the row pass in the spin-ordered (gauge) basis (see GaugeTable).
+  GaugeTable dn_g;
 
   double mean_up_sources = 0.0, mean_dn_sources = 0.0;
   int max_dn_deg = 0, max_up_deg = 0;

@@ -94,14 +94,17 @@ int ftlm_gpu_sector_stats(const ftlm_sector* s, double* mean_up_sources, double*
  * query the sizes. */
 int ftlm_gpu_sector_down_table(const ftlm_sector* s, long long* n_groups, long long* n_entries, long long* gptr,
                                uint32_t* entries, int* pad_hop);
-/* Host copy of the compact row-pass table (inspection and tests; no reference counterpart):
- * *available = 0 when the sector's down hops do not fit its coefficient classes.  Entries
- * src | (lo+1)<<14 | (hi+1)<<19 | dn_sign<<24 | re_class<<25 | im_class<<27 | im_negative<<29,
- * stored [group][round/4][lane][4]; src >= Dd is a zero sentinel (padding).  re4/im4 receive the
- * 4 real parts and |imaginary parts| the classes index.  NULL buffers query the sizes. */
-int ftlm_gpu_sector_down_table_compact(const ftlm_sector* s, int* available, long long* n_groups,
-                                       long long* n_entries, long long* gptr, uint32_t* entries, double* re4,
-                                       double* im4, int* re_bits, int* im_bits);
+/* Host copy of the gauge-basis row-pass table (inspection and tests; no reference counterpart):
+ * *available = 0 when the sector has none (Dd + 8 > 16384, more than 32 sites or more than 512 table
+ * coefficients).  In the basis g(u,d) = (-1)^popc(u & prefix_parity_shifted(d)) a down hop's
+ * coefficient is (-1)^s c_h, s the down-string sign alone.  groups: 4 ints per group of 32 output
+ * down strings (entry offset, real-section rounds KR, table-section rounds KT, 0); round k of lane l
+ * at offset + ((k / 4) * 32 + l) * 4 + k % 4, rounds padded to a multiple of 4.  Real section (k <
+ * KR): src<<4 | cls<<30 | s<<31 with c_h = real2[cls]; table section (KR <= k < KR + KT):
+ * src<<4 | t<<18 | s<<31 with c_h = table[2t] + i table[2t+1].  src >= Dd is a zero sentinel
+ * (padding).  NULL buffers query the sizes. */
+int ftlm_gpu_sector_down_table_gauge(const ftlm_sector* s, int* available, long long* n_groups, long long* n_entries,
+                                     int* n_table, int* groups, uint32_t* entries, double* table, double* real2);
 /* Diagonal entry H[i,i] (host computation from the sector tables). */
 int ftlm_gpu_sector_diag(const ftlm_sector* s, long long index, double* value);
 
@@ -113,11 +116,12 @@ int ftlm_gpu_apply_host(ftlm_sector* s, const double* x_host, double* y_host);
  * = row pass, column-slab pass (one entry for the generic path); *n_passes = entries written. */
 int ftlm_gpu_apply_profiled(ftlm_sector* s, const double* x_dev, double* y_dev, void* stream, float* ms_passes,
                             int* n_passes);
-/* Kernel selection for ftlm_gpu_apply: 0 = automatic, 1 = generic gather, 2 = row+slab passes
- * (row pass with a per-row coefficient table in shared memory), 3 = row+slab passes with the row
- * pass reading register-held coefficient classes from a compact entry table (sectors whose down hops
- * take at most 4 distinct real and 4 distinct |imaginary| coefficient parts; else as 2).  2 and 3
- * give the same sums. */
+/* Kernel selection for ftlm_gpu_apply: 0 = automatic, 1 = generic gather, 2 = row pass (per-row
+ * coefficient table in shared memory) + column-slab pass, 3 = row pass in the gauge basis
+ * (ftlm_gpu_sector_down_table_gauge: register-held real coefficients, one shared-memory load per
+ * hop) + column-slab pass (where the sector has no gauge table, as 2).  Automatic picks 3, else 2,
+ * else 1; ftlm_gpu_autotune_apply times them all.  All paths give the same matrix elements (sums may
+ * differ in the last bits). */
 int ftlm_gpu_set_apply_path(ftlm_sector* s, int path);
 
 /* lanczos_tridiagonal on the sector operator.  alpha/beta: host arrays of max_steps entries;
@@ -202,6 +206,14 @@ int ftlm_gpu_gc_sweep(const ftlm_params* p, int R, int M, unsigned seed, int sta
  * norms in compensated FP64; the M steps of each 32-chain block run as one CUDA graph.  Device
  * memory: 3 block vectors of dim*32 complex64 (127 GB at 4x4 (8,8)), kept between calls until
  * ftlm_gpu_batched_release(). */
+/* Column-pass variant of the batched H·v on this sector: 0/1/2 = 16/8/4-column chunks (the slab of
+ * Du x chunk x 256 bytes that L2 keeps resident while every output row reads it).  Same terms in the
+ * same order per element: the variants give the same block vector. */
+int ftlm_gpu_batched_set_cols_variant(ftlm_sector* s, int variant);
+/* Times the batched H·v with each column-pass variant (CUDA events, reps launches after one warm-up,
+ * on the batched workspace) and keeps the fastest on the sector; the choice is cached per sector shape
+ * for the process (a cached answer returns *ms = -1).  Outputs may be NULL. */
+int ftlm_gpu_batched_autotune(ftlm_sector* s, int reps, int* variant, float* ms);
 /* alpha/beta [R][M] (beta zero-padded after a breakdown), used [R]. */
 int ftlm_gpu_batched_lanczos(ftlm_sector* s, int R, int M, unsigned seed, double* alpha, double* beta, int* used);
 /* ftlm_gpu_ftlm_sector on the batched path; sectors with dim <= 2M use the complex128 path with

@@ -85,3 +85,22 @@ def test_batched_largest_4x4_sectors_within_1e6(gpu, nu, nd):
     print(f"({nu},{nd}): max rel err sector lnZ {rel.max():.2e}; estimate {np.max(err / np.maximum(1.0, np.abs(lz_p))):.2e}")
     assert rel.max() <= 1e-6
     assert np.all(np.isfinite(err)) and np.all(err / np.maximum(1.0, np.abs(lz_p)) <= 1e-6)
+
+
+def test_batched_cols_variants_agree(gpu):
+    """The column-pass variants (16/8/4-column chunks) sum the same terms in the same order per
+    element; only the grouping of the FP64 dot partials differs, so the chains agree to rounding."""
+    s = F.Sector(P44, 4, 4)
+    out = []
+    for v in (0, 1, 2):
+        s.batched_set_cols_variant(v)
+        A, B, used = s.batched_lanczos(32, 8, 11)
+        assert (used == 8).all()
+        out.append((A, B))
+    for A, B in out[1:]:
+        assert np.abs(A - out[0][0]).max() <= 1e-6 * np.abs(out[0][0]).max()
+        assert np.abs(B - out[0][1]).max() <= 1e-6 * np.abs(out[0][1]).max()
+    v, ms = s.batched_autotune(1)
+    assert v in (0, 1, 2) and ms > 0
+    assert F.Sector(P44, 4, 4).batched_autotune(1) == (v, -1.0)  # cached per sector shape
+    F.batched_release()

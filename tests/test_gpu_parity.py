@@ -41,14 +41,14 @@ def test_apply_matches_reference_golden(gpu, golden):
         s = sector_of(c)
         up, dn = s.masks()
         assert np.array_equal(up, g[f"up{k}"]) and np.array_equal(dn, g[f"dn{k}"])
-        for path in (1, 2):
+        for path in (1, 2, 3):
             s.set_apply_path(path)
-            if path == 2 and s.dim() < 64:
+            if path >= 2 and s.dim() < 64:
                 continue
             try:
                 y = s.apply_host(g[f"x{k}"])
             except F.FtlmError as e:
-                assert path == 2 and e.code == _lib.FTLM_ERR_UNSUPPORTED
+                assert path >= 2 and e.code == _lib.FTLM_ERR_UNSUPPORTED
                 continue
             assert relerr(y, g[f"y{k}"]) < RTOL_HV, (c, path)
 
@@ -57,25 +57,31 @@ def test_apply_matches_reference_golden(gpu, golden):
                                (4, 2, 1.0, -0.25, 8.0, 1.0, 0.3, -0.2, 3, 2), (1, 5, 1.0, 0.4, 2.0, 1.5, 0.0, 0.5, 2, 2),
                                (3, 3, 1.0, -0.25, 8.0, 1.0, 0.1, 0.0, 2, 1)])
 def test_matrix_elements_exact(gpu, c):
-    """Dense H from e_j columns: the sparsity pattern and every off-diagonal element (hop
-    coefficient x JW sign) bit-exact against the reference-order oracle; diagonal within 4 ulp."""
+    """Dense H from e_j columns on every H·v path (generic; row pass with the per-row table; row pass
+    in the gauge basis): the sparsity pattern and every off-diagonal element (hop coefficient x JW
+    sign) bit-exact against the reference-order oracle; diagonal within 4 ulp."""
     s = sector_of(c)
     o = O.OracleSector(*c)
     dim = s.dim()
-    Hg = np.zeros((dim, dim), np.complex128)
     Ho = np.zeros((dim, dim), np.complex128)
     e = np.zeros(dim, np.complex128)
     for j in range(dim):
         e[:] = 0
         e[j] = 1.0
-        Hg[:, j] = s.apply_host(e)
         Ho[:, j] = o.apply(e, mode=0)
     off = ~np.eye(dim, dtype=bool)
-    assert np.array_equal(Hg != 0, Ho != 0)
-    assert np.array_equal(Hg[off], Ho[off])
     d = np.diag(Ho).real
-    assert np.all(np.abs(np.diag(Hg).real - d) <= 4 * np.spacing(np.maximum(np.abs(d), 1.0)))
-    assert np.abs(Hg - Hg.conj().T).max() <= 1e-14 * max(1.0, np.abs(Hg).max())  # Hermitian
+    for path in (1, 2, 3) if dim >= 64 else (1,):
+        s.set_apply_path(path)
+        Hg = np.zeros((dim, dim), np.complex128)
+        for j in range(dim):
+            e[:] = 0
+            e[j] = 1.0
+            Hg[:, j] = s.apply_host(e)
+        assert np.array_equal(Hg != 0, Ho != 0), path
+        assert np.array_equal(Hg[off], Ho[off]), path
+        assert np.all(np.abs(np.diag(Hg).real - d) <= 4 * np.spacing(np.maximum(np.abs(d), 1.0)))
+        assert np.abs(Hg - Hg.conj().T).max() <= 1e-14 * max(1.0, np.abs(Hg).max())  # Hermitian
 
 
 @pytest.mark.parametrize("c", [(4, 4, 1.0, -0.25, 8.0, 1.0, 0.1, 0.0, 4, 4), (4, 4, 1.0, -0.25, 8.0, 1.0, 0.1, 0.0, 8, 1),
@@ -88,12 +94,13 @@ def test_paths_agree_and_match_oracle(gpu, c):
     x = rng.standard_normal(dim) + 1j * rng.standard_normal(dim)
     x[rng.random(dim) < 0.02] = 0.0
     ys = []
-    for path in (1, 2):
+    for path in (1, 2, 3):
         s.set_apply_path(path)
         ys.append(s.apply_host(x))
-    assert relerr(ys[1], ys[0]) < RTOL_HV  # the two paths sum the down hops in different orders
     yo = o.apply(x, mode=1, nthreads=8)
-    assert relerr(ys[1], yo) < RTOL_HV
+    for y in ys[1:]:
+        assert relerr(y, ys[0]) < RTOL_HV  # the paths sum the down hops in different orders
+        assert relerr(y, yo) < RTOL_HV
 
 
 def test_tiny_entries_follow_reference_skip_rule(gpu):
@@ -106,13 +113,13 @@ def test_tiny_entries_follow_reference_skip_rule(gpu):
     x = rng.standard_normal(dim) + 1j * rng.standard_normal(dim)
     x[rng.random(dim) < 0.2] = 3e-15 - 2e-15j
     yo = o.apply(x, mode=1, nthreads=8)
-    for path in (1, 2):
+    for path in (1, 2, 3):
         s.set_apply_path(path)
         y = s.apply_host(x)
         assert relerr(y, yo) < RTOL_HV
     # and a vector made only of tiny entries maps to exactly zero
     t = np.full(dim, 1e-15 + 0j)
-    for path in (1, 2):
+    for path in (1, 2, 3):
         s.set_apply_path(path)
         assert not np.any(s.apply_host(t))
 
@@ -327,12 +334,15 @@ def test_lowest_ritz_values_4x4_vs_oracle(gpu):
     import oracle as O
     c = (4, 4, 1.0, -0.25, 8.0, 1.0, 0.1, 0.0, 3, 3)
     s = sector_of(c)
-    a, b, used = s.lanczos(150, 7)
     ao, bo, uo = O.OracleSector(*c).lanczos(150, 7, mode=1, nthreads=16)
-    assert used == uo == 150
-    r_gpu = F.ritz_values(a, b[:149], 5)
     r_cpu = F.ritz_values(ao, bo[:149], 5)
-    assert np.all(np.abs(r_gpu - r_cpu) <= 1e-10 * np.abs(r_cpu)), (r_gpu, r_cpu)
+    for path in (2, 3):  # both fused row + column pass pairs
+        s.set_apply_path(path)
+        a, b, used = s.lanczos(150, 7)
+        assert used == uo == 150
+        r_gpu = F.ritz_values(a, b[:149], 5)
+        assert np.all(np.abs(r_gpu - r_cpu) <= 1e-10 * np.abs(r_cpu)), (path, r_gpu, r_cpu)
+        assert np.all(np.abs(a[:8] - ao[:8]) <= 1e-12 * np.abs(ao[:8])), path
 
 
 def test_error_paths_of_sweep_gradient_and_orbit_entry_points(gpu):
@@ -372,21 +382,23 @@ def test_autotuner_variants_agree(gpu):
     torch = gpu
     s = F.Sector(F.HubbardParams(4, 4, 1.0, -0.25, 8.0, 1.0, 0.1, 0.0), 4, 3)
     x = torch.randn(s.dim(), dtype=torch.complex128, device="cuda")
-    outs = []
-    for v in (0, 1, 2):
-        s.set_apply_path(2)
-        _lib.call("ftlm_gpu_set_cols_variant", s.handle, v)
-        y = torch.empty_like(x)
-        s.apply(x, y)
-        outs.append(y)
+    outs = {}
+    for path in (2, 3):
+        for v in (0, 1, 2):
+            s.set_apply_path(path)
+            _lib.call("ftlm_gpu_set_cols_variant", s.handle, v)
+            y = torch.empty_like(x)
+            s.apply(x, y)
+            outs[path, v] = y
     s.set_apply_path(1)
     yg = torch.empty_like(x)
     s.apply(x, yg)
     torch.cuda.synchronize()
-    assert torch.equal(outs[0], outs[1]) and torch.equal(outs[0], outs[2])
-    assert (outs[0] - yg).abs().max().item() <= RTOL_HV * yg.abs().max().item()
+    for path in (2, 3):
+        assert torch.equal(outs[path, 0], outs[path, 1]) and torch.equal(outs[path, 0], outs[path, 2])
+        assert (outs[path, 0] - yg).abs().max().item() <= RTOL_HV * yg.abs().max().item()
     p, v, ms = s.autotune(2)
-    assert p in (1, 2) and v in (0, 1, 2) and ms > 0
+    assert p in (1, 2, 3) and v in (0, 1, 2) and ms > 0
     y2 = torch.empty_like(x)
     s.apply(x, y2)
     torch.cuda.synchronize()

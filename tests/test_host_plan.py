@@ -172,73 +172,82 @@ def test_down_table_schedule_is_bank_conflict_free(c):
     _lib.lib().ftlm_gpu_sector_destroy(h)
 
 
-def _compact_table(h):
-    ok, ng, ne = C.c_int(), C.c_longlong(), C.c_longlong()
-    _lib.call("ftlm_gpu_sector_down_table_compact", h, C.byref(ok), C.byref(ng), C.byref(ne), None, None, None, None,
+def _gauge_table(h):
+    ok, ng, ne, nt = C.c_int(), C.c_longlong(), C.c_longlong(), C.c_int()
+    _lib.call("ftlm_gpu_sector_down_table_gauge", h, C.byref(ok), C.byref(ng), C.byref(ne), C.byref(nt), None, None,
               None, None)
     if not ok.value:
         return None
-    gptr = np.zeros(ng.value + 1, np.int64)
+    grp = np.zeros(4 * ng.value, np.int32)
     ent = np.zeros(ne.value, np.uint32)
-    re4, im4 = np.zeros(4), np.zeros(4)
-    rb, ib = C.c_int(), C.c_int()
+    tab, real2 = np.zeros(2 * max(nt.value, 1)), np.zeros(2)
     P = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
-    _lib.call("ftlm_gpu_sector_down_table_compact", h, C.byref(ok), C.byref(ng), C.byref(ne), P(gptr), P(ent), P(re4),
-              P(im4), C.byref(rb), C.byref(ib))
-    return gptr, ent, re4, im4
+    _lib.call("ftlm_gpu_sector_down_table_gauge", h, C.byref(ok), C.byref(ng), C.byref(ne), C.byref(nt), P(grp),
+              P(ent), P(tab), P(real2))
+    return grp.reshape(-1, 4), ent, tab[0::2] + 1j * tab[1::2], real2
+
+
+def _prefix_parity_shifted(d):
+    q, par = 0, 0
+    for k in range(32):  # bit k = parity of d's bits in [0, k)
+        q |= par << k
+        par ^= (d >> k) & 1
+    return q
 
 
 @pytest.mark.parametrize("c", [(4, 4, 1.0, -0.25, 8.0, 1.0, 0.1, 0.0, 3, 3), (4, 4, 1.0, -0.25, 8.0, 1.0, 0.0, 0.0, 4, 5),
-                               (4, 3, 1.0, -0.2, 4.0, 1.0, 0.0, 0.0, 3, 4), (3, 3, 1.0, -0.35, 5.75, 0.9, 0.2, 0.0, 4, 4)])
-def test_compact_down_table_reproduces_oracle_row(c):
-    """The compact row-pass encoding (coefficient classes, hop sites for the up-string factor,
-    zero sentinels for padding): decoded on the CPU, the down-hop part of one row plus the diagonal
-    equals the oracle's H x for an x supported on that row (up hops leave the row), to 1e-14; and
-    every round of every quarter-warp, padding included, reads 8 distinct bank groups."""
+                               (4, 3, 1.0, -0.2, 4.0, 1.0, 0.0, 0.0, 3, 4), (3, 3, 1.0, -0.35, 5.75, 0.9, 0.2, 0.1, 4, 4)])
+def test_gauge_down_table_reproduces_oracle_row(c):
+    """The gauge-basis row-pass table, decoded on the CPU: with g(u,d) = (-1)^popc(u & pps(d)), the
+    diagonal plus g * sum_h (-1)^s c_h g x over one row equals the oracle's H x for an x supported on
+    that row (up hops leave the row), to 1e-14; every round of every quarter-warp, padding included,
+    reads 8 distinct bank groups; padding reads the zero sentinels only."""
     Lx, Ly, t, tp, U, V, px, py, nu, nd = c
     hops, pairs = F.build_hubbard_geometry(F.HubbardParams(Lx, Ly, t, tp, U, V, px, py))
     h = C.c_void_p()
     _lib.call("ftlm_gpu_sector_create_host", Lx * Ly, nu, nd, U, V, F.api._c_hops(hops), len(hops),
               F.api._c_pairs(pairs), len(pairs), C.byref(h))
-    tab = _compact_table(h)
+    tab = _gauge_table(h)
     assert tab is not None
-    gptr, ent, re4, im4 = tab
+    grp, ent, table, real2 = tab
     o = O.OracleSector(*c)
     up, dn = o.masks()
     Dd = int(np.count_nonzero(up == up[0]))
+    assert len(grp) == (Dd + 31) // 32
+    pps = np.array([_prefix_parity_shifted(int(d)) for d in dn[:Dd]], dtype=np.int64)
     rng = np.random.default_rng(5)
     for r in (0, (o.dim // Dd) // 2, o.dim // Dd - 1):
         x = np.zeros(o.dim, np.complex128)
         x[r * Dd:(r + 1) * Dd] = rng.standard_normal(Dd) + 1j * rng.standard_normal(Dd)
         ref = o.apply(x, mode=0)[r * Dd:(r + 1) * Dd]
         u = int(up[r * Dd])
-        qu = 0
-        par = 0
-        for k in range(32):  # bit k = parity of u bits in [0, k)
-            qu |= par << k
-            par ^= (u >> k) & 1
-        xs = np.concatenate([x[r * Dd:(r + 1) * Dd], np.zeros(8)])
+        g = np.array([1.0 - 2.0 * (bin(u & int(q)).count("1") & 1) for q in pps])
+        xs = np.concatenate([g * x[r * Dd:(r + 1) * Dd], np.zeros(8)])
         y = np.zeros(Dd, np.complex128)
         v = C.c_double()
         for col in range(Dd):
             _lib.call("ftlm_gpu_sector_diag", h, r * Dd + col, C.byref(v))
-            y[col] = v.value * xs[col]
-        for g in range(len(gptr) - 1):
-            blk = ent[gptr[g]:gptr[g + 1]].reshape(-1, 32, 4).transpose(0, 2, 1).reshape(-1, 32)
+            y[col] = v.value * x[r * Dd + col]
+        for gi, (off, kr, kt, _) in enumerate(grp):
+            k4 = (kr + kt + 3) // 4 * 4
+            blk = ent[off:off + 32 * k4].reshape(k4 // 4, 32, 4).transpose(0, 2, 1).reshape(k4, 32)
+            src = (blk >> 4) & 0x3FFF
             for qw in range(4):
-                for row in blk[:, 8 * qw: 8 * qw + 8] & 0x3FFF:
+                for row in src[:, 8 * qw: 8 * qw + 8]:
                     assert len(set((row % 8).tolist())) == 8
             for l in range(32):
-                col = 32 * g + l
+                col = 32 * gi + l
                 if col >= Dd:
+                    assert np.all(src[:, l] >= Dd)
                     continue
-                for e in blk[:, l].tolist():
-                    src = e & 0x3FFF
-                    if src >= Dd:
+                for k, e in enumerate(blk[:, l].tolist()):
+                    sidx = (e >> 4) & 0x3FFF
+                    if sidx >= Dd:
+                        assert sidx < Dd + 8
                         continue
-                    neg = ((qu >> ((e >> 14) & 31)) ^ (qu >> ((e >> 19) & 31)) ^ (e >> 24)) & 1
-                    cr = re4[(e >> 25) & 3]
-                    ci = im4[(e >> 27) & 3] * (-1.0 if (e >> 29) & 1 else 1.0)
-                    y[col] += (-1.0 if neg else 1.0) * complex(cr, ci) * xs[src]
+                    assert k < kr + kt
+                    cf = real2[(e >> 30) & 1] if k < kr else table[(e >> 18) & 511]
+                    y[col] += (-1.0 if e >> 31 else 1.0) * g[col] * cf * xs[sidx]
         assert np.abs(y - ref).max() <= 1e-14 * np.abs(ref).max()
     _lib.lib().ftlm_gpu_sector_destroy(h)
+
