@@ -61,6 +61,8 @@ def parse():
                     help="hv workload: pin the H·v kernel path (0 = the autotuner's choice)")
     ap.add_argument("--cols-variant", type=int, default=0, choices=[0, 1, 2],
                     help="with --hv-path: column-slab width variant (0/1/2 = 256/128/512 columns)")
+    ap.add_argument("--bt-cols", type=int, default=-1, choices=[-1, 0, 1, 2],
+                    help="batched workload: column-pass variant (-1 = the batched autotuner's choice)")
     ap.add_argument("--check", type=int, default=1,
                     help="sweep workload: chains per sector rerun in complex128 for the per-result error estimate")
     return ap.parse_args()
@@ -395,12 +397,18 @@ def run_batched(args):
     import ftlm_extended_hubbard_b200 as F
     nu, nd = args.sector if args.sector else (NU, ND)
     sec = F.Sector(F.HubbardParams(**PARAMS), nu, nd)
+    if args.bt_cols >= 0:
+        sec.batched_set_cols_variant(args.bt_cols)
+        variant, tuned = args.bt_cols, None
+    else:
+        variant, tuned = sec.batched_autotune()
     sec.batched_lanczos(32, max(1, args.warmup), 7)  # allocation + warm-up
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     sec.batched_lanczos(32, args.steps, 7)
     t = time.perf_counter() - t0
     print(json.dumps({"workload": f"batched Lanczos, 4x4 sector ({nu},{nd}), dim {sec.dim()}, 32 chains",
+                      "cols_variant": variant, "autotune_ms": tuned,
                       "steps": args.steps, "seconds": t, "ms_per_chain_step": 1000.0 * t / (32 * args.steps)}))
     F.batched_release()
     return 0

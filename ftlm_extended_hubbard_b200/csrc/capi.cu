@@ -129,6 +129,10 @@ int upload_plan(ftlm_sector* s) {
     out->ent = ge;
     out->grp = reinterpret_cast<const int4*>(gg);
     out->nt = static_cast<int>(G.tab.size() / 2);
+    out->phase = G.phase ? 1 : 0;
+    out->xor_real = G.xor_real ? 1 : 0;
+    out->pc = G.pc;
+    out->ps = G.ps;
     if (out->nt > 0) {
       double* gt;
       if ((e = upload(G.tab, &gt, &s->owned)) != cudaSuccess) return e;
@@ -320,6 +324,18 @@ int ftlm_gpu_sector_down_table_gauge(const ftlm_sector* s, int* available, long 
   if (entries) std::copy(G.ent.begin(), G.ent.end(), entries);
   if (table) std::copy(G.tab.begin(), G.tab.end(), table);
   if (real2) std::copy(G.real2, G.real2 + 2, real2);
+  return FTLM_OK;
+}
+
+int ftlm_gpu_sector_down_table_form(const ftlm_sector* s, int* phase, double* pc_ps, int* xor_real) {
+  if (!s || !phase) return fail(FTLM_ERR_INVALID, "null argument");
+  const GaugeTable& G = s->plan.dn_g;
+  *phase = (G.ok && G.phase) ? 1 : 0;
+  if (xor_real) *xor_real = (G.ok && G.xor_real) ? 1 : 0;
+  if (pc_ps) {
+    pc_ps[0] = G.pc;
+    pc_ps[1] = G.ps;
+  }
   return FTLM_OK;
 }
 

@@ -12,6 +12,9 @@ struct DevGauge {
   const double2* tab;   // [nt] table-section coefficients
   int nt;
   double real2[2];      // real-section coefficients
+  int phase;            // 1: table-section coefficients are real2[cls] * (pc, +-ps) (entry bits 30, 27)
+  double pc, ps;
+  int xor_real;         // 1: real-section coefficient = real2[0] with its high word ^ (entry & 0xFFFC0000)
 };
 
 struct DevSector {

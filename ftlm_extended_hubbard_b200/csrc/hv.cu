@@ -120,46 +120,71 @@ __device__ __forceinline__ void cmac_xor(double2& acc, double2 c, double2 v, uin
   acc.y = fma(c.y, v.x, acc.y);
 }
 
-// One entry of a gauge table: the real section takes its coefficient from two registers, the table
-// section from the 8-copy table (copy i % 8: the 8 lanes of a quarter-warp hit 8 bank groups).
-__device__ __forceinline__ void gauge_term(double2& acc, uint32_t e, bool real, int i, const unsigned char* line,
-                                           const double2* tab, double a0, double a1) {
+// One real-section entry of a gauge table: the coefficient is one of two register-held values with
+// the entry's sign (cls<<30 | s<<31), or, in the XOR form (kXor), real2[0] with the high word's bits
+// 18..31 flipped by the entry's own bits 18..31 (one XOR: the builder checked that this gives exactly
+// (-1)^s real2[cls]).
+template <bool kXor>
+__device__ __forceinline__ void gauge_real(double2& acc, uint32_t e, const unsigned char* line, double a0, double a1) {
   const double2 v = *reinterpret_cast<const double2*>(line + (e & 0x3FFF0u));
-  if (real) {
+  const double cf = kXor ? __hiloint2double(__double2hiint(a0) ^ static_cast<int>(e & 0xFFFC0000u), __double2loint(a0))
+                         : flip_sign((e & 0x40000000u) ? a1 : a0, e >> 31);
+  acc.x = fma(cf, v.x, acc.x);
+  acc.y = fma(cf, v.y, acc.y);
+}
+
+// One table-section entry: the coefficient from the 8-copy table (copy i % 8: the 8 lanes of a
+// quarter-warp hit 8 bank groups), or, in the phase form (kPhase), real2[cls] times the unit phase
+// (pc, +-ps): the product equals the table value bit for bit (checked when the table is built), so
+// both forms give identical sums, and the phase form spends no shared-memory load on the coefficient.
+template <bool kPhase>
+__device__ __forceinline__ void gauge_cplx(double2& acc, uint32_t e, int i, const unsigned char* line,
+                                           const double2* tab, double a0, double a1, double pc, double ps) {
+  const double2 v = *reinterpret_cast<const double2*>(line + (e & 0x3FFF0u));
+  if (kPhase) {
     const double cf = flip_sign((e & 0x40000000u) ? a1 : a0, e >> 31);
-    acc.x = fma(cf, v.x, acc.x);
-    acc.y = fma(cf, v.y, acc.y);
+    const double cr = cf * pc;
+    const double ci = flip_sign(cf * ps, (e >> 27) & 1u);
+    acc.x = fma(cr, v.x, acc.x);
+    acc.x = fma(-ci, v.y, acc.x);
+    acc.y = fma(cr, v.y, acc.y);
+    acc.y = fma(ci, v.x, acc.y);
   } else {
     cmac_xor(acc, tab[((e >> 18) & 511u) * 8 + (i & 7)], v, e >> 31);
   }
 }
 
 // acc += sum over the gauge-table entries of output string i (one warp = 32 consecutive strings, so
-// the round counts are warp-uniform): 4 rounds per 16-byte load, two loads ahead of their use.
+// the round counts are warp-uniform).  Both sections are whole 4-entry loads, so each runs as its own
+// loop with no per-entry test; entry loads run two ahead of use (the table ends with two padding
+// loads, so the look-ahead needs no bound check).
+template <bool kPhase, bool kXor>
 __device__ __forceinline__ void gauge_hops(double2& acc, const DevGauge& G, int i, const unsigned char* line,
                                            const double2* tab, double a0, double a1) {
   const int4 gp = G.grp[i >> 5];
-  const int kr = gp.y, kt = kr + gp.z;
-  const int nq = (kt + 3) >> 2;
+  const int nr = gp.y >> 2, nq = nr + (gp.z >> 2);
+  const double pc = G.pc, ps = G.ps;
   const uint4* ep = reinterpret_cast<const uint4*>(G.ent + gp.x) + (i & 31);
-  uint4 cur = nq > 0 ? __ldg(ep) : make_uint4(0u, 0u, 0u, 0u);
-  uint4 nxt = nq > 1 ? __ldg(ep + 32) : cur;
-  for (int q = 0; q < nq; ++q) {
+  uint4 cur = __ldg(ep);
+  uint4 nxt = __ldg(ep + 32);
+  int q = 0;
+  for (; q < nr; ++q) {
     const uint4 e = cur;
     cur = nxt;
-    if (q + 2 < nq) nxt = __ldg(ep + (q + 2) * 32);
-    const int k = 4 * q;
-    if (k + 3 < kr) {  // all four in the real section (the common case)
-      gauge_term(acc, e.x, true, i, line, tab, a0, a1);
-      gauge_term(acc, e.y, true, i, line, tab, a0, a1);
-      gauge_term(acc, e.z, true, i, line, tab, a0, a1);
-      gauge_term(acc, e.w, true, i, line, tab, a0, a1);
-    } else {
-      if (k < kt) gauge_term(acc, e.x, k < kr, i, line, tab, a0, a1);
-      if (k + 1 < kt) gauge_term(acc, e.y, k + 1 < kr, i, line, tab, a0, a1);
-      if (k + 2 < kt) gauge_term(acc, e.z, k + 2 < kr, i, line, tab, a0, a1);
-      if (k + 3 < kt) gauge_term(acc, e.w, k + 3 < kr, i, line, tab, a0, a1);
-    }
+    nxt = __ldg(ep + (q + 2) * 32);
+    gauge_real<kXor>(acc, e.x, line, a0, a1);
+    gauge_real<kXor>(acc, e.y, line, a0, a1);
+    gauge_real<kXor>(acc, e.z, line, a0, a1);
+    gauge_real<kXor>(acc, e.w, line, a0, a1);
+  }
+  for (; q < nq; ++q) {
+    const uint4 e = cur;
+    cur = nxt;
+    nxt = __ldg(ep + (q + 2) * 32);
+    gauge_cplx<kPhase>(acc, e.x, i, line, tab, a0, a1, pc, ps);
+    gauge_cplx<kPhase>(acc, e.y, i, line, tab, a0, a1, pc, ps);
+    gauge_cplx<kPhase>(acc, e.z, i, line, tab, a0, a1, pc, ps);
+    gauge_cplx<kPhase>(acc, e.w, i, line, tab, a0, a1, pc, ps);
   }
 }
 
@@ -168,7 +193,9 @@ __device__ __forceinline__ void gauge_hops(double2& acc, const DevGauge& G, int 
 // down-string sign alone, so the row is staged as xs[d] = g(u, d) x[u, d] and every coefficient is
 // the same for all rows: real ones come from two registers (an entry bit picks one), the others from
 // a small table copied once per CTA (8 copies, one per bank group).  Each hop then costs one 16-byte
-// shared load of x (plus one for table hops) instead of two.  Entries: GaugeTable (plan.hpp).
+// shared load of x (plus one for table hops outside the phase form) instead of two.  Entries:
+// GaugeTable (plan.hpp).
+template <bool kPhase, bool kXor>
 __global__ void __launch_bounds__(kRowThreads, 1) hv_rows_gauge_kernel(DevSector S, const double2* __restrict__ x,
                                                                          double2* __restrict__ y, double sx) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -177,7 +204,8 @@ __global__ void __launch_bounds__(kRowThreads, 1) hv_rows_gauge_kernel(DevSector
   double2* tab = xs + Dd + 8;
   const int tid = threadIdx.x;
   const DevGauge G = S.dn_g;
-  for (int i = tid; i < G.nt * 8; i += kRowThreads) tab[i] = G.tab[i >> 3];
+  if (!kPhase)
+    for (int i = tid; i < G.nt * 8; i += kRowThreads) tab[i] = G.tab[i >> 3];
   if (tid < 8) xs[Dd + tid] = make_double2(0.0, 0.0);  // zero sentinels for padding entries
   const double a0 = G.real2[0], a1 = G.real2[1];
   for (int64_t r = blockIdx.x; r < S.Du; r += gridDim.x) {
@@ -209,7 +237,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) hv_rows_gauge_kernel(DevSector
       const double2 xv = xs[c];
       const double dg = diag_value(S, u, S.dmask[c], cuu, S.cnt_dd[c], w);
       double2 acc = make_double2(dg * xv.x, dg * xv.y);
-      gauge_hops(acc, G, c, smem_raw, tab, a0, a1);
+      gauge_hops<kPhase, kXor>(acc, G, c, smem_raw, tab, a0, a1);
       if ((gbits >> j) & 1u) acc = make_double2(-acc.x, -acc.y);
       yrow[c] = acc;
     }
@@ -334,7 +362,7 @@ int g_num_sms = 0;
 }  // namespace
 
 size_t hv_rows_smem_bytes(const DevSector& S) {
-  if (S.dn_g.ent) return static_cast<size_t>(S.Dd + 8 + 8 * S.dn_g.nt) * sizeof(double2);
+  if (S.dn_g.ent) return static_cast<size_t>(S.Dd + 8 + (S.dn_g.phase ? 0 : 8 * S.dn_g.nt)) * sizeof(double2);
   return static_cast<size_t>(S.Dd) * sizeof(double2) + static_cast<size_t>(S.n_dn_hops + 1) * 8 * sizeof(double2);
 }
 
@@ -375,7 +403,9 @@ cudaError_t hv_launch_pass(const DevSector& S, const double2* x, double2* y, int
     cudaError_t e = cudaMemsetAsync(S.flags, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
     const size_t sm = hv_rows_smem_bytes(S);
-    const RowsKernel k = S.dn_g.ent ? hv_rows_gauge_kernel : hv_rows_kernel;
+    const RowsKernel k = !S.dn_g.ent ? hv_rows_kernel
+                         : S.dn_g.phase ? (S.dn_g.xor_real ? hv_rows_gauge_kernel<true, true> : hv_rows_gauge_kernel<true, false>)
+                                        : (S.dn_g.xor_real ? hv_rows_gauge_kernel<false, true> : hv_rows_gauge_kernel<false, false>);
     e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
     if (e != cudaSuccess) return e;
     const int grid_r = static_cast<int>(std::min<int64_t>(S.Du, g_num_sms));

@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cmath>
 #include <complex>
+#include <cstring>
 #include <map>
 #include <utility>
 
@@ -185,6 +186,42 @@ void build_gauge_table(const SpinSpace& sp, const std::vector<MergedHop>& hops, 
   }
   if (nreal == 1) G.real2[1] = G.real2[0];
   if (G.tab.size() / 2 > 512) return;
+  // XOR form of the real section: when the two real values share their low words and their high
+  // words differ only in bits 18..31, the signed coefficient (-1)^s real2[cls] is real2[0] with
+  // bits 18..31 of its high word flipped by the entry's own bits 18..31.
+  {
+    uint64_t b0, b1;
+    std::memcpy(&b0, &G.real2[0], 8);
+    std::memcpy(&b1, &G.real2[1], 8);
+    G.xor_real = static_cast<uint32_t>(b0) == static_cast<uint32_t>(b1) &&
+                 ((static_cast<uint32_t>(b0 >> 32) ^ static_cast<uint32_t>(b1 >> 32)) & 0x3FFFFu) == 0u;
+    G.xor_d = static_cast<uint32_t>(b0 >> 32) ^ static_cast<uint32_t>(b1 >> 32);
+  }
+  // Phase form: find p from the first table value and one of the real values, then require every
+  // table value to be reproduced exactly as real2[k] * (pc, +-ps).
+  const size_t nt = G.tab.size() / 2;
+  std::vector<uint32_t> tab_bits(nt, 0u);  // cls<<30 | conj<<27 per table entry in the phase form
+  for (int k0 = 0; k0 < 2 && nt > 0 && !G.phase; ++k0) {
+    const double a = G.real2[k0];
+    if (a == 0.0) continue;
+    const double pc = G.tab[0] / a, ps = G.tab[1] / a;
+    bool all = true;
+    for (size_t t = 0; t < nt && all; ++t) {
+      bool found = false;
+      for (int k = 0; k < 2 && !found; ++k)
+        for (int cj = 0; cj < 2 && !found; ++cj)
+          if (G.real2[k] * pc == G.tab[2 * t] && G.real2[k] * (cj ? -ps : ps) == G.tab[2 * t + 1]) {
+            tab_bits[t] = (static_cast<uint32_t>(k) << 30) | (static_cast<uint32_t>(cj) << 27);
+            found = true;
+          }
+      all = found;
+    }
+    if (all) {
+      G.phase = true;
+      G.pc = pc;
+      G.ps = ps;
+    }
+  }
   auto sentinel = [D](uint32_t group) {
     return static_cast<uint32_t>(D + static_cast<int64_t>((group + 8u - static_cast<uint32_t>(D & 7)) & 7u)) << 4;
   };
@@ -194,8 +231,10 @@ void build_gauge_table(const SpinSpace& sp, const std::vector<MergedHop>& hops, 
     const uint32_t src = e >> 10, h = (e >> 1) & 511u, sg = e & 1u;
     if (static_cast<int>(h) == nh) return sentinel(src & 7u);
     const int k = cls[h];
+    if (k < 2 && G.xor_real) return (src << 4) | (((k ? G.xor_d : 0u) ^ (sg << 31)) & 0xFFFC0000u);
     if (k < 2) return (src << 4) | (static_cast<uint32_t>(k) << 30) | (sg << 31);
-    return (src << 4) | (static_cast<uint32_t>(k - 2) << 18) | (sg << 31);
+    const uint32_t extra = G.phase ? tab_bits[static_cast<size_t>(k - 2)] : 0u;
+    return (src << 4) | (static_cast<uint32_t>(k - 2) << 18) | extra | (sg << 31);
   };
   const int64_t ngroups = (D + 31) / 32;
   std::vector<std::vector<uint32_t>> lr(32), lt(32), sr(32), st(32);
@@ -224,7 +263,11 @@ void build_gauge_table(const SpinSpace& sp, const std::vector<MergedHop>& hops, 
       KR = std::max(KR, sr[8 * qw].size());
       KT = std::max(KT, st[8 * qw].size());
     }
-    const size_t K4 = (KR + KT + 3) / 4 * 4;
+    // each section padded to whole 4-entry loads: the row pass runs one loop per section with no
+    // per-entry section test
+    KR = (KR + 3) / 4 * 4;
+    KT = (KT + 3) / 4 * 4;
+    const size_t K4 = KR + KT;
     const size_t off = G.ent.size();
     if (off + K4 * 32 > static_cast<size_t>(INT32_MAX)) return;
     G.grp.push_back(static_cast<int32_t>(off));
@@ -246,6 +289,8 @@ void build_gauge_table(const SpinSpace& sp, const std::vector<MergedHop>& hops, 
         G.ent[off + ((k / 4) * 32 + static_cast<size_t>(l)) * 4 + k % 4] = e;
       }
   }
+  // two all-sentinel loads after the last group: the row pass loads two ahead of use unconditionally
+  G.ent.resize(G.ent.size() + 2 * 32 * 4, sentinel(0u));
   G.ok = true;
 }
 

@@ -54,7 +54,8 @@ struct MergedHop {
 // pps(d) = prefix parity of d shifted by one site.  In that basis a hop's coefficient is (-1)^s c_h,
 // s the JW sign of the hopping species' own string alone, so the same table serves every string of
 // the other species.  Built when D + 8 <= 16384, n_sites <= 32 and at most 512 hops need a table
-// coefficient.  Per group of 32 output strings, rounds k = 0 .. KR+KT-1 (padded to a multiple of 4),
+// coefficient.  Per group of 32 output strings, rounds k = 0 .. KR+KT-1 (KR and KT each padded to a
+// multiple of 4 with sentinel rounds),
 // entry of round k for lane l at grp[4g] + ((k / 4) * 32 + l) * 4 + k % 4 (one 16-byte load per
 // lane brings 4 rounds):
 //   real section  (rounds k < KR = grp[4g+1]): hops with c_h = real2[cls], cls in {0, 1};
@@ -64,8 +65,21 @@ struct MergedHop {
 // src << 4 is the byte offset of the 16-byte element in the staged line; src >= D addresses one of 8
 // zero sentinels after it (padding, one per bank group).  Each section is scheduled so that the 8
 // lanes of a quarter-warp read 8 different bank groups in every round.
+// Phase form (phase = true): every table coefficient is one of the two real values times a single
+// unit phase p = (pc, ps) or its conjugate, bit for bit (tab[t] == real2[k] * (pc, +-ps) in double
+// arithmetic) — the case of one Peierls phase, e.g. phi_x != 0 and phi_y == 0.  Table-section entries
+// then also carry cls<<30 and conj<<27, so the row pass forms the coefficient from registers instead
+// of loading it from the shared-memory table (same product, same rounding).
+// XOR form (xor_real = true): real-section entries carry, instead of cls<<30 | s<<31, the bits 18..31
+// by which the high word of (-1)^s real2[cls] differs from that of real2[0] (possible when real2[0]
+// and real2[1] share their low words and their high words differ only in bits 18..31), so the row
+// pass forms the coefficient with one XOR.  Both sections are padded to whole 4-entry loads.
 struct GaugeTable {
   bool ok = false;
+  bool phase = false;
+  bool xor_real = false;
+  uint32_t xor_d = 0;
+  double pc = 1.0, ps = 0.0;
   double real2[2] = {0.0, 0.0};
   std::vector<double> tab;
   std::vector<int32_t> grp;

@@ -99,12 +99,22 @@ int ftlm_gpu_sector_down_table(const ftlm_sector* s, long long* n_groups, long l
  * coefficients).  In the basis g(u,d) = (-1)^popc(u & prefix_parity_shifted(d)) a down hop's
  * coefficient is (-1)^s c_h, s the down-string sign alone.  groups: 4 ints per group of 32 output
  * down strings (entry offset, real-section rounds KR, table-section rounds KT, 0); round k of lane l
- * at offset + ((k / 4) * 32 + l) * 4 + k % 4, rounds padded to a multiple of 4.  Real section (k <
- * KR): src<<4 | cls<<30 | s<<31 with c_h = real2[cls]; table section (KR <= k < KR + KT):
+ * at offset + ((k / 4) * 32 + l) * 4 + k % 4, KR and KT each a multiple of 4.  Real section (k <
+ * KR): src<<4 | cls<<30 | s<<31 with c_h = real2[cls] (or the XOR form, ftlm_gpu_sector_down_table_form);
+ * table section (KR <= k < KR + KT):
  * src<<4 | t<<18 | s<<31 with c_h = table[2t] + i table[2t+1].  src >= Dd is a zero sentinel
  * (padding).  NULL buffers query the sizes. */
 int ftlm_gpu_sector_down_table_gauge(const ftlm_sector* s, int* available, long long* n_groups, long long* n_entries,
                                      int* n_table, int* groups, uint32_t* entries, double* table, double* real2);
+/* Encoding forms of the gauge table (no counterpart in the reference; they say how the row pass
+ * forms each coefficient).  *phase = 1: every table value equals real2[cls] * (pc, +-ps) bit for bit,
+ * with cls = entry bit 30 and the sign of ps from entry bit 27 (set = conjugate), pc_ps[0..1] =
+ * (pc, ps); *phase = 0: the row pass loads table[t] (entry bits 18..26).  *xor_real = 1: a
+ * real-section entry's bits 18..31 are the bits by which the high word of its signed coefficient
+ * (-1)^s real2[cls] differs from that of real2[0] (same low word); *xor_real = 0: cls<<30 | s<<31.
+ * Each section (KR, KT rounds) is padded to a multiple of 4 rounds.  Outputs other than phase may
+ * be NULL. */
+int ftlm_gpu_sector_down_table_form(const ftlm_sector* s, int* phase, double* pc_ps, int* xor_real);
 /* Diagonal entry H[i,i] (host computation from the sector tables). */
 int ftlm_gpu_sector_diag(const ftlm_sector* s, long long index, double* value);
 

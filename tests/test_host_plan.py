@@ -210,6 +210,14 @@ def test_gauge_down_table_reproduces_oracle_row(c):
     tab = _gauge_table(h)
     assert tab is not None
     grp, ent, table, real2 = tab
+    phase, pcps, xor = C.c_int(), np.zeros(2), C.c_int()
+    _lib.call("ftlm_gpu_sector_down_table_form", h, C.byref(phase), pcps.ctypes.data_as(C.c_void_p), C.byref(xor))
+    # one Peierls phase (phi_y == 0, or phi_x == 0) gives the phase form; two phases need the table
+    assert phase.value == (1 if (px == 0.0) != (py == 0.0) else 0)
+    # the XOR form needs the two real values to share their low words (t' = -0.25: -1 and 2 * 0.25)
+    assert xor.value == (1 if tp == -0.25 else 0)
+    a0_bits = int(np.array([real2[0]]).view(np.uint64)[0])
+    assert np.all(grp[:, 1] % 4 == 0) and np.all(grp[:, 2] % 4 == 0)
     o = O.OracleSector(*c)
     up, dn = o.masks()
     Dd = int(np.count_nonzero(up == up[0]))
@@ -247,7 +255,16 @@ def test_gauge_down_table_reproduces_oracle_row(c):
                         continue
                     assert k < kr + kt
                     cf = real2[(e >> 30) & 1] if k < kr else table[(e >> 18) & 511]
-                    y[col] += (-1.0 if e >> 31 else 1.0) * g[col] * cf * xs[sidx]
+                    sign = -1.0 if e >> 31 else 1.0
+                    if k < kr and xor.value:  # (-1)^s real2[cls]: real2[0] with high-word bits ^ e
+                        cf = float(np.array([a0_bits ^ ((e & 0xFFFC0000) << 32)], np.uint64).view(np.float64)[0])
+                        assert cf in (real2[0], -real2[0], real2[1], -real2[1])
+                        sign = 1.0
+                    if k >= kr and phase.value:  # the row pass forms it as real2[cls] * (pc, +-ps)
+                        a = real2[(e >> 30) & 1]
+                        pf = complex(a * pcps[0], a * (-pcps[1] if (e >> 27) & 1 else pcps[1]))
+                        assert pf == cf, (pf, cf)
+                    y[col] += sign * g[col] * cf * xs[sidx]
         assert np.abs(y - ref).max() <= 1e-14 * np.abs(ref).max()
     _lib.lib().ftlm_gpu_sector_destroy(h)
 
