@@ -141,6 +141,16 @@ int upload_plan(ftlm_sector* s) {
     return cudaSuccess;
   };
   CU_TRY(upload_gauge(P.dn_g, &D.dn_g));
+  D.up_pk = nullptr;
+  D.up_real2[0] = P.up_real2[0];
+  D.up_real2[1] = P.up_real2[1];
+  D.up_pc = P.up_pc;
+  D.up_ps = P.up_ps;
+  if (P.up_pk_ok) {
+    uint32_t* upk;
+    CU_TRY(upload(P.up_pk, &upk, &s->owned));
+    D.up_pk = upk;
+  }
   D.umask = um;
   D.dmask = dm;
   D.cnt_uu = cuu;
@@ -335,6 +345,23 @@ int ftlm_gpu_sector_down_table_form(const ftlm_sector* s, int* phase, double* pc
   if (pc_ps) {
     pc_ps[0] = G.pc;
     pc_ps[1] = G.ps;
+  }
+  return FTLM_OK;
+}
+
+int ftlm_gpu_sector_up_table_packed(const ftlm_sector* s, int* available, long long* n_entries, int32_t* ptr,
+                                    uint32_t* entries, double* real2, double* pc_ps) {
+  if (!s || !available || !n_entries) return fail(FTLM_ERR_INVALID, "null argument");
+  const SectorPlan& P = s->plan;
+  *available = P.up_pk_ok ? 1 : 0;
+  *n_entries = P.up_pk_ok ? static_cast<long long>(P.up_pk.size()) : 0;
+  if (!P.up_pk_ok) return FTLM_OK;
+  if (ptr) std::copy(P.up_ptr.begin(), P.up_ptr.end(), ptr);
+  if (entries) std::copy(P.up_pk.begin(), P.up_pk.end(), entries);
+  if (real2) std::copy(P.up_real2, P.up_real2 + 2, real2);
+  if (pc_ps) {
+    pc_ps[0] = P.up_pc;
+    pc_ps[1] = P.up_ps;
   }
   return FTLM_OK;
 }

@@ -170,8 +170,9 @@ struct ftlm_sector {
     if (stream) cudaStreamDestroy(stream);
   }
   // Kernel choice for H·v: 1 = generic gather; 2 = row pass with the per-row coefficient table +
-  // column-slab pass; 3 = row pass in the gauge basis (register-held real coefficients) + column-slab
-  // pass.  Automatic: 3, else 2, else 1.
+  // column-slab pass over the CSR up list; 3 = row pass in the gauge basis (register-held real
+  // coefficients) + column-slab pass over the packed up list where the sector has one.  Automatic:
+  // 3, else 2, else 1.
   bool path_available(int path) const {
     if (path == 1) return true;
     if (path == 3 && !dev.dn_g.ent) return false;
@@ -182,10 +183,14 @@ struct ftlm_sector {
     if (path_available(3)) return 3;
     return path_available(2) ? 2 : 1;
   }
-  // The device view a launch of `path` uses (the row pass reads dn_g on path 3 only).
+  // The device view a launch of `path` uses (the row pass reads dn_g, the column pass up_pk, on
+  // path 3 only).
   ftlm_b200::DevSector dev_for(int path) const {
     ftlm_b200::DevSector d = dev;
-    if (path != 3) d.dn_g.ent = nullptr;
+    if (path != 3) {
+      d.dn_g.ent = nullptr;
+      d.up_pk = nullptr;
+    }
     return d;
   }
   int apply(const double2* x, double2* y, cudaStream_t st) {

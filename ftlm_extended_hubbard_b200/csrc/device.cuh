@@ -30,6 +30,11 @@ struct DevSector {
   const int32_t* up_src;   // [nnz_up]
   const double2* up_coef;  // [nnz_up]
   const uint32_t* up_lohi; // [nnz_up]
+  // Packed up list of the column pass (SectorPlan::up_pk), nullptr when the sector has none:
+  // src | lo<<14 | hi<<19 | conj<<28 | phase<<29 | cls<<30 | s<<31.
+  const uint32_t* up_pk;   // [nnz_up]
+  double up_real2[2];
+  double up_pc, up_ps;
   const int64_t* dn_gptr;  // [ngroups+1]
   const uint32_t* dn_ent;  // ELL entries
   const int64_t* dn_csr_ptr;   // [Dd+1] unpadded down-hop lists (batched path)

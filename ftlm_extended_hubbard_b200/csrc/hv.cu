@@ -310,33 +310,131 @@ __device__ __forceinline__ void cols_body(const DevSector& S, const double2* __r
   if (has1) y[r * S.Dd + c1] = acc1;
 }
 
-template <int kColThreads, bool kFused>
+// The column pass over the packed up list (SectorPlan::up_pk): one 4-byte word per source, read
+// four at a time from shared memory, gives the source row, the (lo, hi) of the column-dependent sign
+// and the coefficient (-1)^s real2[cls] (times (pc, +-ps) for a phase hop).  A real coefficient costs
+// two FMAs per column instead of a complex multiply, and the list costs a quarter of a shared load per
+// source instead of three.  The kind of each source is the same for every thread of the block, so
+// the phase test does not diverge.  Same products and sums as cols_body on the CSR list.
+template <int kColThreads, bool kFilter, bool kFused>
+__device__ __forceinline__ void cols_body_packed(const DevSector& S, const double2* __restrict__ x,
+                                                 double2* __restrict__ y, int64_t r, int64_t c0, int deg,
+                                                 const uint32_t* s_pk, double sx, double (&dot)[2]) {
+  const int64_t c1 = c0 + kColThreads;
+  const bool has1 = c1 < S.Dd;
+  const int64_t c1s = has1 ? c1 : c0;
+  const uint32_t q0 = prefix_parity_shifted(S.dmask[c0]);
+  const uint32_t q1 = prefix_parity_shifted(S.dmask[c1s]);
+  double2* y0 = y + r * S.Dd + c0;
+  double2 acc0 = kFused ? make_double2(0.0, 0.0) : *y0;
+  double2 acc1 = (has1 && !kFused) ? y[r * S.Dd + c1] : make_double2(0.0, 0.0);
+  const double2* x0 = x + c0;
+  const double2* x1 = x + c1s;
+  const int64_t Dd = S.Dd;
+  const double a0 = S.up_real2[0], a1 = S.up_real2[1], pc = S.up_pc, ps = S.up_ps;
+  auto skip = [sx](double2 v) { return kFused ? tiny(make_double2(sx * v.x, sx * v.y)) : tiny(v); };
+  auto term = [&](uint32_t pk, double2 v0, double2 v1) {
+    const uint32_t lo = (pk >> 14) & 31u, hi = (pk >> 19) & 31u;
+    const double cf = flip_sign((pk & 0x40000000u) ? a1 : a0, pk >> 31);
+    const uint32_t f0 = ((q0 >> lo) ^ (q0 >> hi)) & 1u, f1 = ((q1 >> lo) ^ (q1 >> hi)) & 1u;
+    if (pk & 0x20000000u) {  // phase hop: cf * (pc, +-ps), the column sign on both parts
+      const double cr = cf * pc;
+      const double ci = flip_sign(cf * ps, (pk >> 28) & 1u);
+      const double2 c = make_double2(cr, ci);
+      if (!kFilter || !skip(v0)) cmac_xor(acc0, c, v0, f0);
+      if (!kFilter || !skip(v1)) cmac_xor(acc1, c, v1, f1);
+    } else {
+      if (!kFilter || !skip(v0)) {
+        const double c = flip_sign(cf, f0);
+        acc0.x = fma(c, v0.x, acc0.x);
+        acc0.y = fma(c, v0.y, acc0.y);
+      }
+      if (!kFilter || !skip(v1)) {
+        const double c = flip_sign(cf, f1);
+        acc1.x = fma(c, v1.x, acc1.x);
+        acc1.y = fma(c, v1.y, acc1.y);
+      }
+    }
+  };
+  int j = 0;
+  for (; j + 4 <= deg; j += 4) {
+    const uint4 pk = *reinterpret_cast<const uint4*>(s_pk + j);
+    const uint32_t p[4] = {pk.x, pk.y, pk.z, pk.w};
+    double2 v0[4], v1[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int64_t off = static_cast<int64_t>(p[t] & 0x3FFFu) * Dd;
+      v0[t] = x0[off];
+      v1[t] = x1[off];
+    }
+#pragma unroll
+    for (int t = 0; t < 4; ++t) term(p[t], v0[t], v1[t]);
+  }
+  for (; j < deg; ++j) {
+    const uint32_t pk = s_pk[j];
+    const int64_t off = static_cast<int64_t>(pk & 0x3FFFu) * Dd;
+    term(pk, x0[off], x1[off]);
+  }
+  if constexpr (kFused) {
+    const double2 r0 = *y0;
+    acc0 = make_double2(fma(sx, acc0.x, r0.x), fma(sx, acc0.y, r0.y));
+    const double2 xq0 = x[r * S.Dd + c0];
+    const double qx = sx * xq0.x, qy = sx * xq0.y;  // conj(q) * y
+    dot[0] += qx * acc0.x + qy * acc0.y;
+    dot[1] += qx * acc0.y - qy * acc0.x;
+    if (has1) {
+      const double2 r1 = y[r * S.Dd + c1];
+      acc1 = make_double2(fma(sx, acc1.x, r1.x), fma(sx, acc1.y, r1.y));
+      const double2 xq1 = x[r * S.Dd + c1];
+      const double px = sx * xq1.x, py = sx * xq1.y;
+      dot[0] += px * acc1.x + py * acc1.y;
+      dot[1] += px * acc1.y - py * acc1.x;
+    }
+  }
+  *y0 = acc0;
+  if (has1) y[r * S.Dd + c1] = acc1;
+}
+
+template <int kColThreads, bool kFused, bool kPacked>
 __global__ void __launch_bounds__(kColThreads) hv_cols_kernel(DevSector S, const double2* __restrict__ x,
                                                               double2* __restrict__ y, double sx,
                                                               double* __restrict__ dotp) {
   constexpr int kColChunk = 2 * kColThreads;
-  __shared__ int64_t s_off[kMaxUpDeg];
-  __shared__ double2 s_coef[kMaxUpDeg];
-  __shared__ uint32_t s_lh[kMaxUpDeg];
+  constexpr int kListDeg = kPacked ? 4 : kMaxUpDeg;  // the list arrays of the form this launch does not use
+  __shared__ int64_t s_off[kListDeg];
+  __shared__ double2 s_coef[kListDeg];
+  __shared__ uint32_t s_lh[kListDeg];
+  __shared__ __align__(16) uint32_t s_pk[kPacked ? kMaxUpDeg : 4];
   const int64_t b = blockIdx.x;
   const int64_t chunk = b / S.Du;
   const int64_t r = b - chunk * S.Du;
   const int j0 = S.up_ptr[r];
   const int deg = S.up_ptr[r + 1] - j0;
   for (int j = threadIdx.x; j < deg; j += kColThreads) {
-    s_off[j] = static_cast<int64_t>(S.up_src[j0 + j]) * S.Dd;
-    s_coef[j] = S.up_coef[j0 + j];
-    s_lh[j] = S.up_lohi[j0 + j];
+    if constexpr (kPacked) {
+      s_pk[j] = S.up_pk[j0 + j];
+    } else {
+      s_off[j] = static_cast<int64_t>(S.up_src[j0 + j]) * S.Dd;
+      s_coef[j] = S.up_coef[j0 + j];
+      s_lh[j] = S.up_lohi[j0 + j];
+    }
   }
   const bool filt = (*S.flags) != 0;
   __syncthreads();
   const int64_t c0 = chunk * kColChunk + threadIdx.x;
   double dot[2] = {0.0, 0.0};
   if (c0 < S.Dd) {
-    if (filt)
-      cols_body<kColThreads, true, kFused>(S, x, y, r, c0, deg, s_off, s_coef, s_lh, sx, dot);
-    else
-      cols_body<kColThreads, false, kFused>(S, x, y, r, c0, deg, s_off, s_coef, s_lh, sx, dot);
+    if constexpr (kPacked) {
+      if (filt)
+        cols_body_packed<kColThreads, true, kFused>(S, x, y, r, c0, deg, s_pk, sx, dot);
+      else
+        cols_body_packed<kColThreads, false, kFused>(S, x, y, r, c0, deg, s_pk, sx, dot);
+    } else {
+      if (filt)
+        cols_body<kColThreads, true, kFused>(S, x, y, r, c0, deg, s_off, s_coef, s_lh, sx, dot);
+      else
+        cols_body<kColThreads, false, kFused>(S, x, y, r, c0, deg, s_off, s_coef, s_lh, sx, dot);
+    }
   }
   if constexpr (kFused) {  // fixed tree over the block: one (re, im) partial per block
     __shared__ double red[2][kColThreads];
@@ -383,10 +481,18 @@ template <int kThreads>
 cudaError_t launch_cols(const DevSector& S, const double2* x, double2* y, cudaStream_t st, double sx, double* dotp) {
   const int64_t nchunks = (S.Dd + 2 * kThreads - 1) / (2 * kThreads);
   const unsigned grid = static_cast<unsigned>(nchunks * S.Du);
-  if (dotp || sx != 1.0)
-    hv_cols_kernel<kThreads, true><<<grid, kThreads, 0, st>>>(S, x, y, sx, dotp);
-  else
-    hv_cols_kernel<kThreads, false><<<grid, kThreads, 0, st>>>(S, x, y, sx, dotp);
+  const bool fused = dotp || sx != 1.0;
+  if (S.up_pk) {
+    if (fused)
+      hv_cols_kernel<kThreads, true, true><<<grid, kThreads, 0, st>>>(S, x, y, sx, dotp);
+    else
+      hv_cols_kernel<kThreads, false, true><<<grid, kThreads, 0, st>>>(S, x, y, sx, dotp);
+  } else {
+    if (fused)
+      hv_cols_kernel<kThreads, true, false><<<grid, kThreads, 0, st>>>(S, x, y, sx, dotp);
+    else
+      hv_cols_kernel<kThreads, false, false><<<grid, kThreads, 0, st>>>(S, x, y, sx, dotp);
+  }
   return cudaGetLastError();
 }
 

@@ -400,6 +400,78 @@ double plan_diag(const SectorPlan& p, int64_t ru, int64_t rd) {
   return p.U * static_cast<double>(popc(u & d)) + p.V * static_cast<double>(vcount);
 }
 
+namespace {
+
+// Packed up-hop list (see SectorPlan::up_pk): every merged up hop's coefficient must be one of two
+// real values, or one of them times a single unit phase p or its conjugate, exactly.
+void build_up_packed(SectorPlan* Pp) {
+  SectorPlan& P = *Pp;
+  P.up_pk_ok = false;
+  P.up_pk.clear();
+  if (P.up.D > (1 << 14) || P.n > 32) return;
+  const int nh = static_cast<int>(P.hu.size());
+  std::vector<uint32_t> hbits(static_cast<size_t>(nh), 0u);  // cls<<30 | phase<<29 | conj<<28
+  int nreal = 0;
+  for (int h = 0; h < nh && nreal <= 2; ++h) {
+    const MergedHop& m = P.hu[static_cast<size_t>(h)];
+    if (m.cim != 0.0) continue;
+    int k = -1;
+    for (int i = 0; i < nreal; ++i)
+      if (P.up_real2[i] == m.cre) k = i;
+    if (k < 0) {
+      if (nreal == 2) return;
+      P.up_real2[nreal] = m.cre;
+      k = nreal++;
+    }
+    hbits[static_cast<size_t>(h)] = static_cast<uint32_t>(k) << 30;
+  }
+  if (nreal == 1) P.up_real2[1] = P.up_real2[0];
+  // p from the first complex hop and one of the real values; every complex hop must then be
+  // real2[k] * (pc, +-ps) exactly
+  int first = -1;
+  for (int h = 0; h < nh && first < 0; ++h)
+    if (P.hu[static_cast<size_t>(h)].cim != 0.0) first = h;
+  bool all = true;
+  for (int k0 = 0; k0 < 2 && first >= 0; ++k0) {
+    const double a = P.up_real2[k0];
+    if (a == 0.0) continue;
+    P.up_pc = P.hu[static_cast<size_t>(first)].cre / a;
+    P.up_ps = P.hu[static_cast<size_t>(first)].cim / a;
+    all = true;
+    for (int h = 0; h < nh && all; ++h) {
+      const MergedHop& m = P.hu[static_cast<size_t>(h)];
+      if (m.cim == 0.0) continue;
+      bool found = false;
+      for (int k = 0; k < 2 && !found; ++k)
+        for (int cj = 0; cj < 2 && !found; ++cj)
+          if (P.up_real2[k] * P.up_pc == m.cre && P.up_real2[k] * (cj ? -P.up_ps : P.up_ps) == m.cim) {
+            hbits[static_cast<size_t>(h)] = (static_cast<uint32_t>(k) << 30) | (1u << 29) | (static_cast<uint32_t>(cj) << 28);
+            found = true;
+          }
+      all = found;
+    }
+    if (all) break;
+  }
+  if (!all) return;
+  P.up_pk.reserve(P.up_src.size());
+  for (int64_t r = 0; r < P.up.D; ++r) {
+    const uint32_t u2 = P.up.masks[static_cast<size_t>(r)];
+    for (int h = 0; h < nh; ++h) {  // the CSR builder's order
+      const MergedHop& m = P.hu[static_cast<size_t>(h)];
+      if (!((u2 >> m.to) & 1u) || ((u2 >> m.from) & 1u)) continue;
+      const uint32_t u = u2 ^ (1u << m.from) ^ (1u << m.to);
+      const uint32_t src = static_cast<uint32_t>(P.up.rank(u));
+      const uint32_t sg = static_cast<uint32_t>(popc(u & m.own_mask) & 1);
+      P.up_pk.push_back(src | (static_cast<uint32_t>(m.lo) << 14) | (static_cast<uint32_t>(m.hi) << 19) |
+                        hbits[static_cast<size_t>(h)] | (sg << 31));
+    }
+  }
+  P.up_pk_ok = P.up_pk.size() == P.up_src.size();
+  if (!P.up_pk_ok) P.up_pk.clear();
+}
+
+}  // namespace
+
 std::string build_plan(int n_sites, int n_up, int n_dn, double U, double V, const std::vector<HopIn>& hops,
                        const std::vector<PairIn>& pairs, SectorPlan* out) {
   init_binom();
@@ -481,6 +553,7 @@ std::string build_plan(int n_sites, int n_up, int n_dn, double U, double V, cons
     P.up_ptr[static_cast<size_t>(r) + 1] = static_cast<int32_t>(P.up_src.size());
   }
   P.mean_up_sources = P.up.D ? static_cast<double>(P.up_src.size()) / static_cast<double>(P.up.D) : 0.0;
+  build_up_packed(&P);
 
   // Down part: per output down string d', hop f->t contributes from d = d' ^ f ^ t; the
   // down-string factor (-1)^#dn(lo,hi) goes into the entry, the up-string factor per row.

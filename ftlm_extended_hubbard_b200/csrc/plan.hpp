@@ -103,6 +103,13 @@ struct SectorPlan {
   std::vector<int32_t> up_ptr, up_src;
   std::vector<double> up_coef;  // 2 per entry
   std::vector<uint32_t> up_lohi;
+  // The same list packed into one word per entry for the column pass (built when Du <= 16384, at
+  // most 32 sites, and every coefficient is (-1)^s real2[cls], or that times (pc, +-ps) for one unit
+  // phase, bit for bit): src | lo<<14 | hi<<19 | conj<<28 | phase<<29 | cls<<30 | s<<31.
+  bool up_pk_ok = false;
+  double up_real2[2] = {0.0, 0.0};
+  double up_pc = 1.0, up_ps = 0.0;
+  std::vector<uint32_t> up_pk;
 
   // Down part (ELL, 32 consecutive output down ranks per group, entry k of lane l at
   // dn_gptr[g] + 32k + l): entry = src_rank<<10 | hop_id<<1 | dn_string_sign.  Padding

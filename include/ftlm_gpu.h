@@ -115,6 +115,15 @@ int ftlm_gpu_sector_down_table_gauge(const ftlm_sector* s, int* available, long 
  * Each section (KR, KT rounds) is padded to a multiple of 4 rounds.  Outputs other than phase may
  * be NULL. */
 int ftlm_gpu_sector_down_table_form(const ftlm_sector* s, int* phase, double* pc_ps, int* xor_real);
+/* Host copy of the packed up-hop list of the column pass (inspection and tests; no reference
+ * counterpart): *available = 0 when the sector has none (Du > 16384, more than 32 sites, or a
+ * coefficient outside the form below; the column pass then reads the CSR list).  ptr: Du + 1
+ * offsets; entry = src | lo<<14 | hi<<19 | conj<<28 | phase<<29 | cls<<30 | s<<31: output up string
+ * r gathers x[src, c] with coefficient (-1)^s real2[cls] (times (pc, +-ps), minus sign when conj,
+ * for a phase hop) and the column sign (-1)^(number of down sites of column c in [lo, hi)).  NULL
+ * buffers query the size. */
+int ftlm_gpu_sector_up_table_packed(const ftlm_sector* s, int* available, long long* n_entries, int32_t* ptr,
+                                    uint32_t* entries, double* real2, double* pc_ps);
 /* Diagonal entry H[i,i] (host computation from the sector tables). */
 int ftlm_gpu_sector_diag(const ftlm_sector* s, long long index, double* value);
 

@@ -268,3 +268,51 @@ def test_gauge_down_table_reproduces_oracle_row(c):
         assert np.abs(y - ref).max() <= 1e-14 * np.abs(ref).max()
     _lib.lib().ftlm_gpu_sector_destroy(h)
 
+
+
+@pytest.mark.parametrize("c", [(4, 4, 1.0, -0.25, 8.0, 1.0, 0.1, 0.0, 3, 3), (4, 3, 1.0, -0.2, 4.0, 1.0, 0.0, 0.0, 3, 4),
+                               (3, 3, 1.0, -0.35, 5.75, 0.9, 0.2, 0.1, 4, 4)])
+def test_packed_up_list_reproduces_oracle_columns(c):
+    """The column pass's packed up list, decoded on the CPU: for x supported on one column c, the
+    oracle's (H x)[:, c] minus the diagonal equals sum_j (-1)^s real2[cls] [p or conj p] times the
+    column sign (-1)^(#down sites of c in [lo, hi)) times x[src_j, c] (up hops keep the column), to
+    1e-14; a lattice with two Peierls phases has no packed list."""
+    Lx, Ly, t, tp, U, V, px, py, nu, nd = c
+    hops, pairs = F.build_hubbard_geometry(F.HubbardParams(Lx, Ly, t, tp, U, V, px, py))
+    h = C.c_void_p()
+    _lib.call("ftlm_gpu_sector_create_host", Lx * Ly, nu, nd, U, V, F.api._c_hops(hops), len(hops),
+              F.api._c_pairs(pairs), len(pairs), C.byref(h))
+    ok, ne = C.c_int(), C.c_longlong()
+    _lib.call("ftlm_gpu_sector_up_table_packed", h, C.byref(ok), C.byref(ne), None, None, None, None)
+    assert ok.value == (0 if (px != 0.0 and py != 0.0) else 1)
+    if not ok.value:
+        _lib.lib().ftlm_gpu_sector_destroy(h)
+        return
+    o = O.OracleSector(*c)
+    up, dn = o.masks()
+    Dd = int(np.count_nonzero(up == up[0]))
+    Du = o.dim // Dd
+    ptr = np.zeros(Du + 1, np.int32)
+    ent = np.zeros(ne.value, np.uint32)
+    real2, pcps = np.zeros(2), np.zeros(2)
+    P = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    _lib.call("ftlm_gpu_sector_up_table_packed", h, C.byref(ok), C.byref(ne), P(ptr), P(ent), P(real2), P(pcps))
+    rng = np.random.default_rng(11)
+    for col in (0, Dd // 2, Dd - 1):
+        x = np.zeros(o.dim, np.complex128)
+        x[col::Dd] = rng.standard_normal(Du) + 1j * rng.standard_normal(Du)
+        ref = o.apply(x, mode=0)[col::Dd]
+        d = int(dn[col])
+        y = np.zeros(Du, np.complex128)
+        v = C.c_double()
+        for r in range(Du):
+            _lib.call("ftlm_gpu_sector_diag", h, r * Dd + col, C.byref(v))
+            y[r] = v.value * x[r * Dd + col]
+            for e in ent[ptr[r]:ptr[r + 1]].tolist():
+                src, lo, hi = e & 0x3FFF, (e >> 14) & 31, (e >> 19) & 31
+                a = real2[(e >> 30) & 1] * (-1.0 if e >> 31 else 1.0)
+                cf = complex(a * pcps[0], a * (-pcps[1] if (e >> 28) & 1 else pcps[1])) if (e >> 29) & 1 else a
+                colsign = -1.0 if bin(d & ((1 << hi) - (1 << lo))).count("1") & 1 else 1.0
+                y[r] += colsign * cf * x[src * Dd + col]
+        assert np.abs(y - ref).max() <= 1e-14 * np.abs(ref).max()
+    _lib.lib().ftlm_gpu_sector_destroy(h)
