@@ -156,35 +156,51 @@ __device__ __forceinline__ void gauge_cplx(double2& acc, uint32_t e, int i, cons
 
 // acc += sum over the gauge-table entries of output string i (one warp = 32 consecutive strings, so
 // the round counts are warp-uniform).  Both sections are whole 4-entry loads, so each runs as its own
-// loop with no per-entry test; entry loads run two ahead of use (the table ends with two padding
-// loads, so the look-ahead needs no bound check).
+// loop with no per-entry test; the last load of a section holds kr % 4 (kt % 4) rounds before its
+// padding, and only those are gathered.  Entry loads run two ahead of use (the table ends with two
+// padding loads, so the look-ahead needs no bound check).
 template <bool kPhase, bool kXor>
 __device__ __forceinline__ void gauge_hops(double2& acc, const DevGauge& G, int i, const unsigned char* line,
                                            const double2* tab, double a0, double a1) {
   const int4 gp = G.grp[i >> 5];
-  const int nr = gp.y >> 2, nq = nr + (gp.z >> 2);
+  const int kr = gp.w & 0xFFFF, kt = gp.w >> 16;  // rounds before the padding to whole loads
   const double pc = G.pc, ps = G.ps;
   const uint4* ep = reinterpret_cast<const uint4*>(G.ent + gp.x) + (i & 31);
   uint4 cur = __ldg(ep);
   uint4 nxt = __ldg(ep + 32);
   int q = 0;
-  for (; q < nr; ++q) {
+  auto next = [&]() {
     const uint4 e = cur;
     cur = nxt;
     nxt = __ldg(ep + (q + 2) * 32);
+    ++q;
+    return e;
+  };
+  for (int n = kr >> 2; n > 0; --n) {
+    const uint4 e = next();
     gauge_real<kXor>(acc, e.x, line, a0, a1);
     gauge_real<kXor>(acc, e.y, line, a0, a1);
     gauge_real<kXor>(acc, e.z, line, a0, a1);
     gauge_real<kXor>(acc, e.w, line, a0, a1);
   }
-  for (; q < nq; ++q) {
-    const uint4 e = cur;
-    cur = nxt;
-    nxt = __ldg(ep + (q + 2) * 32);
+  if (kr & 3) {
+    const uint4 e = next();
+    gauge_real<kXor>(acc, e.x, line, a0, a1);
+    if ((kr & 3) > 1) gauge_real<kXor>(acc, e.y, line, a0, a1);
+    if ((kr & 3) > 2) gauge_real<kXor>(acc, e.z, line, a0, a1);
+  }
+  for (int n = kt >> 2; n > 0; --n) {
+    const uint4 e = next();
     gauge_cplx<kPhase>(acc, e.x, i, line, tab, a0, a1, pc, ps);
     gauge_cplx<kPhase>(acc, e.y, i, line, tab, a0, a1, pc, ps);
     gauge_cplx<kPhase>(acc, e.z, i, line, tab, a0, a1, pc, ps);
     gauge_cplx<kPhase>(acc, e.w, i, line, tab, a0, a1, pc, ps);
+  }
+  if (kt & 3) {
+    const uint4 e = next();
+    gauge_cplx<kPhase>(acc, e.x, i, line, tab, a0, a1, pc, ps);
+    if ((kt & 3) > 1) gauge_cplx<kPhase>(acc, e.y, i, line, tab, a0, a1, pc, ps);
+    if ((kt & 3) > 2) gauge_cplx<kPhase>(acc, e.z, i, line, tab, a0, a1, pc, ps);
   }
 }
 

@@ -264,16 +264,17 @@ void build_gauge_table(const SpinSpace& sp, const std::vector<MergedHop>& hops, 
       KT = std::max(KT, st[8 * qw].size());
     }
     // each section padded to whole 4-entry loads: the row pass runs one loop per section with no
-    // per-entry section test
+    // per-entry section test, and skips the padding rounds of each section's last load
+    const size_t KR0 = KR, KT0 = KT;
     KR = (KR + 3) / 4 * 4;
     KT = (KT + 3) / 4 * 4;
     const size_t K4 = KR + KT;
     const size_t off = G.ent.size();
-    if (off + K4 * 32 > static_cast<size_t>(INT32_MAX)) return;
+    if (off + K4 * 32 > static_cast<size_t>(INT32_MAX) || KR0 > 0xFFFF || KT0 > 0x7FFF) return;
     G.grp.push_back(static_cast<int32_t>(off));
     G.grp.push_back(static_cast<int32_t>(KR));
     G.grp.push_back(static_cast<int32_t>(KT));
-    G.grp.push_back(0);
+    G.grp.push_back(static_cast<int32_t>(KR0 | (KT0 << 16)));
     // round k of lane l at off + ((k / 4) * 32 + l) * 4 + k % 4: a lane loads 4 rounds with one
     // 16-byte load.  Rounds a quarter does not need, and the rounds that pad the group to a
     // multiple of 4: lane l reads the sentinel of bank group l % 8.

@@ -54,8 +54,9 @@ struct MergedHop {
 // pps(d) = prefix parity of d shifted by one site.  In that basis a hop's coefficient is (-1)^s c_h,
 // s the JW sign of the hopping species' own string alone, so the same table serves every string of
 // the other species.  Built when D + 8 <= 16384, n_sites <= 32 and at most 512 hops need a table
-// coefficient.  Per group of 32 output strings, rounds k = 0 .. KR+KT-1 (KR and KT each padded to a
-// multiple of 4 with sentinel rounds),
+// coefficient.  Per group of 32 output strings (grp[4g..4g+3] = entry offset, KR, KT, KR0 | KT0<<16),
+// rounds k = 0 .. KR+KT-1 (KR and KT each padded to a multiple of 4 with sentinel rounds; KR0 and KT0
+// are the rounds before that padding),
 // entry of round k for lane l at grp[4g] + ((k / 4) * 32 + l) * 4 + k % 4 (one 16-byte load per
 // lane brings 4 rounds):
 //   real section  (rounds k < KR = grp[4g+1]): hops with c_h = real2[cls], cls in {0, 1};

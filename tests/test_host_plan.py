@@ -236,10 +236,13 @@ def test_gauge_down_table_reproduces_oracle_row(c):
         for col in range(Dd):
             _lib.call("ftlm_gpu_sector_diag", h, r * Dd + col, C.byref(v))
             y[col] = v.value * x[r * Dd + col]
-        for gi, (off, kr, kt, _) in enumerate(grp):
+        for gi, (off, kr, kt, k0) in enumerate(grp):
             k4 = (kr + kt + 3) // 4 * 4
             blk = ent[off:off + 32 * k4].reshape(k4 // 4, 32, 4).transpose(0, 2, 1).reshape(k4, 32)
             src = (blk >> 4) & 0x3FFF
+            kr0, kt0 = k0 & 0xFFFF, k0 >> 16  # rounds before the padding to whole loads: the rest is padding
+            assert kr0 <= kr < kr0 + 4 and kt0 <= kt < kt0 + 4
+            assert np.all(src[kr0:kr] >= Dd) and np.all(src[kr + kt0:kr + kt] >= Dd)
             for qw in range(4):
                 for row in src[:, 8 * qw: 8 * qw + 8]:
                     assert len(set((row % 8).tolist())) == 8
