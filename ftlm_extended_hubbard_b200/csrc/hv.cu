@@ -411,8 +411,10 @@ __device__ __forceinline__ void cols_body_packed(const DevSector& S, const doubl
   if (has1) y[r * S.Dd + c1] = acc1;
 }
 
+// At least 896 resident threads per SM (28 warps): the L2 gathers need the bytes in flight, and the
+// fused form would otherwise take a few registers more and drop to 24 warps.
 template <int kColThreads, bool kFused, bool kPacked>
-__global__ void __launch_bounds__(kColThreads) hv_cols_kernel(DevSector S, const double2* __restrict__ x,
+__global__ void __launch_bounds__(kColThreads, 896 / kColThreads) hv_cols_kernel(DevSector S, const double2* __restrict__ x,
                                                               double2* __restrict__ y, double sx,
                                                               double* __restrict__ dotp) {
   constexpr int kColChunk = 2 * kColThreads;
@@ -452,21 +454,29 @@ __global__ void __launch_bounds__(kColThreads) hv_cols_kernel(DevSector S, const
         cols_body<kColThreads, false, kFused>(S, x, y, r, c0, deg, s_off, s_coef, s_lh, sx, dot);
     }
   }
-  if constexpr (kFused) {  // fixed tree over the block: one (re, im) partial per block
-    __shared__ double red[2][kColThreads];
-    red[0][threadIdx.x] = dot[0];
-    red[1][threadIdx.x] = dot[1];
-    __syncthreads();
-    for (int h = kColThreads / 2; h > 0; h >>= 1) {
-      if (static_cast<int>(threadIdx.x) < h) {
-        red[0][threadIdx.x] += red[0][threadIdx.x + h];
-        red[1][threadIdx.x] += red[1][threadIdx.x + h];
-      }
-      __syncthreads();
+  if constexpr (kFused) {  // fixed tree over the block (warp shuffles, then warps in order): one partial
+    constexpr int kWarps = kColThreads / 32;
+    __shared__ double red[2][kWarps];
+#pragma unroll
+    for (int h = 16; h > 0; h >>= 1) {
+      dot[0] += __shfl_down_sync(0xFFFFFFFFu, dot[0], h);
+      dot[1] += __shfl_down_sync(0xFFFFFFFFu, dot[1], h);
     }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+      red[0][warp] = dot[0];
+      red[1][warp] = dot[1];
+    }
+    __syncthreads();
     if (threadIdx.x == 0 && dotp) {
-      dotp[2 * b] = red[0][0];
-      dotp[2 * b + 1] = red[1][0];
+      double s0 = red[0][0], s1 = red[1][0];
+#pragma unroll
+      for (int w = 1; w < kWarps; ++w) {
+        s0 += red[0][w];
+        s1 += red[1][w];
+      }
+      dotp[2 * b] = s0;
+      dotp[2 * b + 1] = s1;
     }
   }
 }
