@@ -59,8 +59,9 @@ def parse():
     ap.add_argument("--k", type=int, nargs=2, default=(1, 2), metavar=("KX", "KY"), help="orbit workload momentum")
     ap.add_argument("--hv-path", type=int, default=0, choices=[0, 1, 2, 3],
                     help="hv workload: pin the H·v kernel path (0 = the autotuner's choice)")
-    ap.add_argument("--cols-variant", type=int, default=0, choices=[0, 1, 2],
-                    help="with --hv-path: column-slab width variant (0/1/2 = 256/128/512 columns)")
+    ap.add_argument("--cols-variant", type=int, default=0, choices=[0, 1, 2, 3, 4, 5],
+                    help="with --hv-path: column-slab width variant (0/1/2 = 256/128/512 columns; "
+                         "3/4/5 = the same over the packed up list, path 3)")
     ap.add_argument("--bt-cols", type=int, default=-1, choices=[-1, 0, 1, 2],
                     help="batched workload: column-pass variant (-1 = the batched autotuner's choice)")
     ap.add_argument("--check", type=int, default=1,
@@ -362,7 +363,8 @@ def run_ours(args):
                    "vector": "torch.randn complex128, seed 7+rank",
                    "l2": "inputs larger than L2 (2.65 GB per vector); no flush",
                    "parallelism": f"independent H·v per rank x{ws}",
-                   "hv_variant": {"path": tuned_path, "cols_slab": [256, 128, 512][tuned_cols], "chosen_by": chosen_by}},
+                   "hv_variant": {"path": tuned_path, "cols_slab": [256, 128, 512][tuned_cols % 3],
+                                  "up_list": "packed" if tuned_cols >= 3 else "csr", "chosen_by": chosen_by}},
         "gpu_launches": 2 * args.steps,
         "kernels_ms": {"hv_rows": rows_avg, "hv_cols": cols_avg},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",

@@ -987,7 +987,7 @@ int ftlm_gpu_lanczos_sectors(ftlm_sector* const* secs, int n_sectors, int R, int
 }
 
 int ftlm_gpu_set_cols_variant(ftlm_sector* s, int variant) {
-  if (!s || variant < 0 || variant > 2) return fail(FTLM_ERR_INVALID, "cols variant must be 0, 1 or 2");
+  if (!s || variant < 0 || variant > 5) return fail(FTLM_ERR_INVALID, "cols variant must be in [0, 6)");
   s->cols_variant = variant;
   return FTLM_OK;
 }
@@ -1029,12 +1029,13 @@ int ftlm_gpu_autotune_apply(ftlm_sector* s, int reps, int* path, int* cols_varia
   int best_p = 1, best_v = 0;
   float best = 3.4e38f;
   const bool fast = hv_fast_path_ok(s->dev_for(2), P.max_up_deg);
-  const int variants[7][2] = {{1, 0}, {2, 0}, {2, 1}, {2, 2}, {3, 0}, {3, 1}, {3, 2}};
+  const int variants[10][2] = {{1, 0}, {2, 0}, {2, 1}, {2, 2}, {3, 0}, {3, 1}, {3, 2}, {3, 3}, {3, 4}, {3, 5}};
   cudaError_t ce = cudaSuccess;
   for (const auto& v : variants) {
     if (v[0] >= 2 && !fast) continue;
     if (v[0] == 3 && !s->path_available(3)) continue;
-    const DevSector d = s->dev_for(v[0]);
+    if (v[1] >= 3 && !s->dev.up_pk) continue;
+    const DevSector d = s->dev_for(v[0], v[1]);
     const int lp = v[0] == 3 ? 2 : v[0];
     ce = hv_launch(d, x.as<double2>(), y.as<double2>(), lp, st, v[1]);  // warm-up
     if (ce == cudaSuccess) ce = cudaEventRecord(e0, st);

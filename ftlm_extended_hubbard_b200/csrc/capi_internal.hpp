@@ -161,7 +161,7 @@ struct ftlm_sector {
   ftlm_b200::DevSector dev{};
   std::vector<void*> owned;
   int apply_path = 0;    // 0 auto, 1 generic, 2 rows+cols, 3 rows (register coefficient classes)+cols
-  int cols_variant = 0;  // column-slab width of path 2 (hv_launch)
+  int cols_variant = 0;  // column slab 256/128/512 (0/1/2); 3/4/5: the same over the packed up list (path 3)
   ftlm_b200::capi::LanczosWs ws;
   ftlm_b200::capi::DevBuf hx, hy;  // staging for the host-buffer apply
   cudaStream_t stream = nullptr;
@@ -171,8 +171,8 @@ struct ftlm_sector {
   }
   // Kernel choice for H·v: 1 = generic gather; 2 = row pass with the per-row coefficient table +
   // column-slab pass over the CSR up list; 3 = row pass in the gauge basis (register-held real
-  // coefficients) + column-slab pass over the packed up list where the sector has one.  Automatic:
-  // 3, else 2, else 1.
+  // coefficients) + column-slab pass, over the packed up list when cols_variant >= 3 and the sector
+  // has one.  Automatic: 3, else 2, else 1.
   bool path_available(int path) const {
     if (path == 1) return true;
     if (path == 3 && !dev.dn_g.ent) return false;
@@ -183,14 +183,13 @@ struct ftlm_sector {
     if (path_available(3)) return 3;
     return path_available(2) ? 2 : 1;
   }
-  // The device view a launch of `path` uses (the row pass reads dn_g, the column pass up_pk, on
-  // path 3 only).
-  ftlm_b200::DevSector dev_for(int path) const {
+  // The device view a launch of `path` with column variant cv uses (the row pass reads dn_g on path
+  // 3 only, the column pass up_pk on path 3 with cv >= 3 only).
+  ftlm_b200::DevSector dev_for(int path, int cv = -1) const {
     ftlm_b200::DevSector d = dev;
-    if (path != 3) {
-      d.dn_g.ent = nullptr;
-      d.up_pk = nullptr;
-    }
+    if (cv < 0) cv = cols_variant;
+    if (path != 3) d.dn_g.ent = nullptr;
+    if (path != 3 || cv < 3) d.up_pk = nullptr;
     return d;
   }
   int apply(const double2* x, double2* y, cudaStream_t st) {

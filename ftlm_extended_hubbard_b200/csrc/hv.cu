@@ -523,6 +523,7 @@ cudaError_t launch_cols(const DevSector& S, const double2* x, double2* y, cudaSt
 }
 
 int64_t hv_cols_blocks(const DevSector& S, int cols_variant) {
+  cols_variant %= 3;  // 3..5: the same slabs over the packed list
   const int threads = cols_variant == 1 ? 64 : (cols_variant == 2 ? 256 : 128);
   return (S.Dd + 2 * threads - 1) / (2 * threads) * S.Du;
 }
@@ -544,6 +545,7 @@ cudaError_t hv_launch_pass(const DevSector& S, const double2* x, double2* y, int
     k<<<grid_r, kRowThreads, sm, st>>>(S, x, y, sx);
     return cudaGetLastError();
   }
+  cols_variant %= 3;  // 3..5: the same slabs; the list form comes with S (S.up_pk)
   if (cols_variant == 1) return launch_cols<64>(S, x, y, st, sx, dotp);
   if (cols_variant == 2) return launch_cols<256>(S, x, y, st, sx, dotp);
   return launch_cols<128>(S, x, y, st, sx, dotp);

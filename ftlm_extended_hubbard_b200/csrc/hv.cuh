@@ -8,8 +8,9 @@
 namespace ftlm_b200 {
 
 // path: 1 = generic gather kernel, 2 = row pass + column-slab pass.  The row pass reads the gauge
-// table when S.dn_g.ent is set (else the per-row coefficient table).  cols_variant: column slab of
-// 256 (0), 128 (1) or 512 (2) columns.
+// table when S.dn_g.ent is set (else the per-row coefficient table), the column pass the packed up
+// list when S.up_pk is set (else the CSR list).  cols_variant: column slab of 256 (0 or 3), 128 (1
+// or 4) or 512 (2 or 5) columns.
 cudaError_t hv_launch(const DevSector& S, const double2* x, double2* y, int path, cudaStream_t st,
                       int cols_variant = 0);
 // One pass of the fast path: 0 = row pass (diag + down hops), 1 = column-slab pass (up hops).

@@ -266,13 +266,15 @@ int ftlm_gpu_batched_release(void);
  * No reference counterpart (scheduling only). */
 int ftlm_gpu_set_fused_max_dim(long long max_dim);
 /* Autotuner (no reference counterpart): times the sector's H·v variants — the generic gather kernel
- * and, where it fits, the row + column-slab pair with 256-, 128- and 512-column slabs (and the
- * register-class row pass with 256-column slabs) — `reps` times
+ * and, where it fits, both row passes with 256-, 128- and 512-column slabs (the gauge row pass also
+ * with the packed up list) — `reps` times
  * each on a device vector and keeps the fastest for this handle (later ftlm_gpu_apply calls use it).
  * The choice is cached per sector shape (sites, particle numbers, hop counts) for the process; a
  * cached answer returns *ms = -1.  Outputs may be NULL.  Replaces ftlm_gpu_set_apply_path's choice. */
 int ftlm_gpu_autotune_apply(ftlm_sector* s, int reps, int* path, int* cols_variant, float* ms);
-/* Column-slab width of the row + column pair: 0 = 256, 1 = 128, 2 = 512 columns. */
+/* Column-slab width of the row + column pair: 0 = 256, 1 = 128, 2 = 512 columns over the CSR up list;
+ * 3 / 4 / 5 = the same widths over the packed up list (ftlm_gpu_sector_up_table_packed; path 3 only,
+ * else as 0 / 1 / 2). */
 int ftlm_gpu_set_cols_variant(ftlm_sector* s, int variant);
 /* The Lanczos chains of several sectors in one launch (one CTA per chain, all M steps on the device):
  * chain r of sector i uses seed + r*100003 and start_mode as ftlm_gpu_lanczos; alpha/beta

@@ -71,15 +71,16 @@ def test_matrix_elements_exact(gpu, c):
         Ho[:, j] = o.apply(e, mode=0)
     off = ~np.eye(dim, dtype=bool)
     d = np.diag(Ho).real
-    for path in (1, 2, 3) if dim >= 64 else (1,):
-        s.set_apply_path(path)
+    for path, cv in ((1, 0), (2, 0), (3, 0), (3, 3)) if dim >= 64 else ((1, 0),):
+        s.set_apply_path(path)  # path 3 with the CSR (0) and the packed (3) up list
+        _lib.call("ftlm_gpu_set_cols_variant", s.handle, cv)
         Hg = np.zeros((dim, dim), np.complex128)
         for j in range(dim):
             e[:] = 0
             e[j] = 1.0
             Hg[:, j] = s.apply_host(e)
-        assert np.array_equal(Hg != 0, Ho != 0), path
-        assert np.array_equal(Hg[off], Ho[off]), path
+        assert np.array_equal(Hg != 0, Ho != 0), (path, cv)
+        assert np.array_equal(Hg[off], Ho[off]), (path, cv)
         assert np.all(np.abs(np.diag(Hg).real - d) <= 4 * np.spacing(np.maximum(np.abs(d), 1.0)))
         assert np.abs(Hg - Hg.conj().T).max() <= 1e-14 * max(1.0, np.abs(Hg).max())  # Hermitian
 
@@ -377,14 +378,15 @@ def test_error_paths_of_sweep_gradient_and_orbit_entry_points(gpu):
 
 
 def test_autotuner_variants_agree(gpu):
-    """Every H·v variant the autotuner chooses from gives the same vector: the column-slab widths
-    bitwise (same terms, same order per element), the generic kernel within rounding."""
+    """Every H·v variant the autotuner chooses from gives the same vector: the column-slab widths and
+    the CSR or packed up list bitwise (same terms, same products, same order per element), the
+    generic kernel within rounding."""
     torch = gpu
     s = F.Sector(F.HubbardParams(4, 4, 1.0, -0.25, 8.0, 1.0, 0.1, 0.0), 4, 3)
     x = torch.randn(s.dim(), dtype=torch.complex128, device="cuda")
     outs = {}
     for path in (2, 3):
-        for v in (0, 1, 2):
+        for v in range(6):
             s.set_apply_path(path)
             _lib.call("ftlm_gpu_set_cols_variant", s.handle, v)
             y = torch.empty_like(x)
@@ -395,10 +397,10 @@ def test_autotuner_variants_agree(gpu):
     s.apply(x, yg)
     torch.cuda.synchronize()
     for path in (2, 3):
-        assert torch.equal(outs[path, 0], outs[path, 1]) and torch.equal(outs[path, 0], outs[path, 2])
+        assert all(torch.equal(outs[path, 0], outs[path, v]) for v in range(1, 6)), path
         assert (outs[path, 0] - yg).abs().max().item() <= RTOL_HV * yg.abs().max().item()
     p, v, ms = s.autotune(2)
-    assert p in (1, 2, 3) and v in (0, 1, 2) and ms > 0
+    assert p in (1, 2, 3) and v in range(6) and ms > 0
     y2 = torch.empty_like(x)
     s.apply(x, y2)
     torch.cuda.synchronize()
