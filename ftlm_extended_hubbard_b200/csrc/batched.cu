@@ -16,6 +16,7 @@
 //     the vector update evaluated in FP64 and rounded to complex64;
 //   * every kernel is persistent with a fixed grid (kBtBlocks) and fixed per-block work order, so
 //     the FP64 reductions are bitwise repeatable.
+#include <algorithm>
 #include <cstdio>
 
 #include "batched.cuh"
@@ -220,6 +221,131 @@ __global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_rows_kernel(Dev
   }
 }
 
+// Staged row pass (the default where the sector has the gauge-basis row table, plan.hpp GaugeTable):
+// one work item = (up row r, chain pair p).  The row's slice of the two chains, W[r, :, 2p..2p+1]
+// (16 bytes per basis state, 206 KB at 4x4 (8,8)), is staged in shared memory, and the down hops are
+// gathered there with the complex128 row pass's table and schedule (the same 16-byte element size,
+// so the same bank-group-free rounds): one 16-byte shared load serves two chains, instead of the
+// 256-byte L2 gather of bt_rows_kernel for 32 chains.  Coefficients are the double-precision table
+// values rounded to FP32 (what bt_rows_kernel's signed FP32 table holds); sums in FP32.
+constexpr int kBtsThreads = 1024;
+
+__device__ __forceinline__ double flip_d(double v, uint32_t neg) {
+  return __hiloint2double(__double2hiint(v) ^ static_cast<int>(neg << 31), __double2loint(v));
+}
+
+template <bool kXor>
+__device__ __forceinline__ void bts_real(float4& acc, uint32_t e, const unsigned char* line, double a0, double a1) {
+  const float4 v = *reinterpret_cast<const float4*>(line + (e & 0x3FFF0u));
+  const double cd = kXor ? __hiloint2double(__double2hiint(a0) ^ static_cast<int>(e & 0xFFFC0000u), __double2loint(a0))
+                         : flip_d((e & 0x40000000u) ? a1 : a0, e >> 31);
+  const float c = __double2float_rn(cd);
+  acc.x = fmaf(c, v.x, acc.x);
+  acc.y = fmaf(c, v.y, acc.y);
+  acc.z = fmaf(c, v.z, acc.z);
+  acc.w = fmaf(c, v.w, acc.w);
+}
+
+// Complex-section entry: the coefficient from the CTA's copy of the table in FP32 (8 copies, copy i % 8:
+// the 8 lanes of a quarter-warp read 8 different bank groups), with the entry's sign.
+__device__ __forceinline__ void bts_cplx(float4& acc, uint32_t e, int i, const unsigned char* line, const float2* tab) {
+  const float4 v = *reinterpret_cast<const float4*>(line + (e & 0x3FFF0u));
+  float2 c = tab[((e >> 18) & 511u) * 8 + (i & 7)];
+  const uint32_t f = (e >> 31) << 31;
+  c = make_float2(__uint_as_float(__float_as_uint(c.x) ^ f), __uint_as_float(__float_as_uint(c.y) ^ f));
+  cmac4(acc, c, v, 0u);
+}
+
+// The gauge-table walk of hv.cu's row pass for output string i (sections as whole 4-entry loads, the
+// padding rounds of each section's last load skipped, entry loads two ahead of use).
+template <bool kXor>
+__device__ __forceinline__ void bts_hops(float4& acc, const DevGauge& G, int i, const unsigned char* line,
+                                         const float2* tab, double a0, double a1) {
+  const int4 gp = G.grp[i >> 5];
+  const int kr = gp.w & 0xFFFF, kt = gp.w >> 16;
+  const uint4* ep = reinterpret_cast<const uint4*>(G.ent + gp.x) + (i & 31);
+  uint4 cur = __ldg(ep);
+  uint4 nxt = __ldg(ep + 32);
+  int q = 0;
+  auto next = [&]() {
+    const uint4 e = cur;
+    cur = nxt;
+    nxt = __ldg(ep + (q + 2) * 32);
+    ++q;
+    return e;
+  };
+  for (int n = kr >> 2; n > 0; --n) {
+    const uint4 e = next();
+    bts_real<kXor>(acc, e.x, line, a0, a1);
+    bts_real<kXor>(acc, e.y, line, a0, a1);
+    bts_real<kXor>(acc, e.z, line, a0, a1);
+    bts_real<kXor>(acc, e.w, line, a0, a1);
+  }
+  if (kr & 3) {
+    const uint4 e = next();
+    bts_real<kXor>(acc, e.x, line, a0, a1);
+    if ((kr & 3) > 1) bts_real<kXor>(acc, e.y, line, a0, a1);
+    if ((kr & 3) > 2) bts_real<kXor>(acc, e.z, line, a0, a1);
+  }
+  for (int n = kt >> 2; n > 0; --n) {
+    const uint4 e = next();
+    bts_cplx(acc, e.x, i, line, tab);
+    bts_cplx(acc, e.y, i, line, tab);
+    bts_cplx(acc, e.z, i, line, tab);
+    bts_cplx(acc, e.w, i, line, tab);
+  }
+  if (kt & 3) {
+    const uint4 e = next();
+    bts_cplx(acc, e.x, i, line, tab);
+    if ((kt & 3) > 1) bts_cplx(acc, e.y, i, line, tab);
+    if ((kt & 3) > 2) bts_cplx(acc, e.z, i, line, tab);
+  }
+}
+
+template <bool kXor>
+__global__ void __launch_bounds__(kBtsThreads, 1) bt_rows_staged_kernel(DevSector S, const float2* __restrict__ W,
+                                                                         float2* __restrict__ Y,
+                                                                         const int* __restrict__ flag) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int Dd = static_cast<int>(S.Dd);
+  float4* xs = reinterpret_cast<float4*>(smem_raw);
+  float2* tab = reinterpret_cast<float2*>(xs + Dd + 8);
+  const int tid = threadIdx.x;
+  const DevGauge G = S.dn_g;
+  const bool filter = *flag != 0;
+  for (int i = tid; i < G.nt * 8; i += kBtsThreads) {
+    const double2 c = G.tab[i >> 3];
+    tab[i] = make_float2(__double2float_rn(c.x), __double2float_rn(c.y));
+  }
+  if (tid < 8) xs[Dd + tid] = make_float4(0.f, 0.f, 0.f, 0.f);  // zero sentinels for padding entries
+  const double a0 = G.real2[0], a1 = G.real2[1];
+  const float4* W4 = reinterpret_cast<const float4*>(W);
+  float4* Y4 = reinterpret_cast<float4*>(Y);
+  const int64_t items = S.Du * (kBtChains / 2);
+  for (int64_t it = blockIdx.x; it < items; it += gridDim.x) {
+    const int64_t r = it / (kBtChains / 2);
+    const int p = static_cast<int>(it - r * (kBtChains / 2));
+    const uint32_t u = S.umask[r];
+    const int cuu = S.cnt_uu[r];
+    const uint4 wp = S.wpl[r];
+    const int64_t base = r * S.Dd * (kBtChains / 2) + p;  // float4 index of state (r, 0), chains 2p, 2p+1
+    for (int c = tid; c < Dd; c += kBtsThreads) {
+      float4 v = W4[base + static_cast<int64_t>(c) * (kBtChains / 2)];
+      if (filter) v = filt4(v);
+      xs[c] = v;
+    }
+    __syncthreads();
+    for (int c = tid; c < Dd; c += kBtsThreads) {
+      const float4 xv = xs[c];
+      const float dg = static_cast<float>(diag_value(S, u, S.dmask[c], cuu, S.cnt_dd[c], wp));
+      float4 acc = make_float4(dg * xv.x, dg * xv.y, dg * xv.z, dg * xv.w);
+      bts_hops<kXor>(acc, G, c, smem_raw, tab, a0, a1);
+      Y4[base + static_cast<int64_t>(c) * (kBtChains / 2)] = acc;
+    }
+    __syncthreads();
+  }
+}
+
 // Gathers of the orbit pass: two half-warps take every other source of the warp's list.
 template <bool kFilter>
 __device__ __forceinline__ float4 bt_cols_sum(const float4* Wc, const uint32_t* s_off, const float2* s_cf, int deg8,
@@ -339,6 +465,29 @@ __global__ void __launch_bounds__(kBtThreads, kBtBlocksPerSm) bt_cols_kernel(Dev
     partial[(blockIdx.x * 32 + chain) * 2] = re;
     partial[(blockIdx.x * 32 + chain) * 2 + 1] = im;
   }
+}
+
+// Row pass of the batched H·V: the staged kernel where the sector has the gauge table and the
+// staged slice fits shared memory, else bt_rows_kernel.
+cudaError_t launch_bt_rows(const DevSector& S, const float2* W, float2* Y, const int* flag, cudaStream_t s) {
+  if (S.dn_g.ent) {
+    const size_t sm = static_cast<size_t>(S.Dd + 8) * sizeof(float4) + static_cast<size_t>(S.dn_g.nt) * 8 * sizeof(float2);
+    if (sm <= 227 * 1024) {
+      using K = void (*)(DevSector, const float2*, float2*, const int*);
+      const K k = S.dn_g.xor_real ? bt_rows_staged_kernel<true> : bt_rows_staged_kernel<false>;
+      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
+      if (e != cudaSuccess) return e;
+      int dev = 0, nsm = 148;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      const int64_t items = S.Du * (kBtChains / 2);
+      const int grid = static_cast<int>(std::min<int64_t>(items, nsm));
+      k<<<grid, kBtsThreads, sm, s>>>(S, W, Y, flag);
+      return cudaGetLastError();
+    }
+  }
+  bt_rows_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(S, W, Y, flag);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_bt_cols(int cols_variant, const DevSector& S, const float2* W, float2* Y, double* partial,
@@ -606,7 +755,7 @@ cudaError_t bt_step(const DevSector& S, const float2* Wk, const float2* Wkm1, fl
   int* fout = flags + ((k + 1) & 1);
   cudaError_t e = cudaMemsetAsync(fout, 0, sizeof(int), s);
   if (e != cudaSuccess) return e;
-  bt_rows_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(S, Wk, Y, fin);
+  launch_bt_rows(S, Wk, Y, fin, s);
   launch_bt_cols(S.bt_cols, S, Wk, Y, partial, fin, s);
   bt_scalar_kernel<<<1, 32, 0, s>>>(partial, kBtBlocks, 1, k, st, alpha, beta, used);
   bt_update_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(Y, Wk, Wkm1, S.dim, st, k > 0, partial, fout);
@@ -630,7 +779,7 @@ cudaError_t bt_orbit_step(const OrbitApplyDev& A, const float2* Wk, const float2
 cudaError_t bt_apply(const DevSector& S, const float2* X, float2* Y, const double* st_unit, double* partial,
                      const int* zero_flag, cudaStream_t s) {
   (void)st_unit;
-  bt_rows_kernel<<<kBtBlocks, kBtThreads, 0, s>>>(S, X, Y, zero_flag);
+  launch_bt_rows(S, X, Y, zero_flag, s);
   launch_bt_cols(S.bt_cols, S, X, Y, partial, zero_flag, s);
   return cudaGetLastError();
 }
