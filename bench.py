@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--sector", type=int, nargs=2, default=None, metavar=("NU", "ND"),
                     help="profile a smaller 4x4 sector instead (for ncu captures); not a bench line")
-    ap.add_argument("--workload", default="hv", choices=["hv", "batched", "sweep-model", "orbit", "grad", "kresolved", "published", "sweep"],
+    ap.add_argument("--workload", default="hv", choices=["hv", "batched", "lanczos", "sweep-model", "orbit", "grad", "kresolved", "published", "sweep"],
                     help="hv: the H·v benchmark (the bench line).  Measurement aids (one JSON line each, not "
                          "bench lines): batched = 32-chain complex64 Lanczos steps on one sector; sweep-model = "
                          "per-sector step cost of the plain and batched paths over the full 4x4 sweep (R=32, "
@@ -416,6 +416,30 @@ def run_batched(args):
     return 0
 
 
+def run_lanczos(args):
+    """Plain complex128 Lanczos step on one 4x4 sector (the fused recurrence of ftlm_gpu_lanczos, Philox
+    start, the autotuned H·v variant): wall time per step from a (warmup + steps)-step chain minus a
+    warmup-step chain, so start-vector and set-up costs cancel."""
+    import torch
+    import ftlm_extended_hubbard_b200 as F
+    nu, nd = args.sector if args.sector else (NU, ND)
+    sec = F.Sector(F.HubbardParams(**PARAMS), nu, nd)
+    path, cols, _ = sec.autotune(3)
+    w = max(1, args.warmup)
+    sec.lanczos(w, 7, start="philox")
+    times = []
+    for m in (w, w + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sec.lanczos(m, 7, start="philox")
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    print(json.dumps({"workload": f"plain complex128 Lanczos, 4x4 sector ({nu},{nd}), dim {sec.dim()}",
+                      "hv_variant": {"path": path, "cols_variant": cols}, "steps": args.steps,
+                      "ms_per_step": 1e3 * (times[1] - times[0]) / args.steps}))
+    return 0
+
+
 def run_sweep_model(args):
     """Per-sector Lanczos step cost of both paths on every 4x4 sector class (dims equal under
     N -> 16-N and spin exchange), combined into the time of a full R=32, M=100 sweep."""
@@ -622,6 +646,8 @@ def main():
         return run_reference(args)
     if args.workload == "batched":
         return run_batched(args)
+    if args.workload == "lanczos":
+        return run_lanczos(args)
     if args.workload == "sweep-model":
         return run_sweep_model(args)
     if args.workload == "orbit":
