@@ -73,7 +73,7 @@ SIGNATURES = {
     "ftlm_gpu_sector_diag": [_vp, _ll, _pd],
     "ftlm_gpu_sector_down_table": [_vp, C.POINTER(_ll), C.POINTER(_ll), _vp, _vp, _pi],
     "ftlm_gpu_sector_down_table_gauge": [_vp, _pi, C.POINTER(_ll), C.POINTER(_ll), _pi, _vp, _vp, _vp, _vp],
-    "ftlm_gpu_sector_down_table_form": [_vp, _pi, _vp, _pi],
+    "ftlm_gpu_sector_down_table_form": [_vp, _pi, _vp, _pi, _vp],
     "ftlm_gpu_sector_up_table_packed": [_vp, _pi, C.POINTER(_ll), _vp, _vp, _vp, _vp],
     "ftlm_gpu_apply": [_vp, _vp, _vp, _vp],
     "ftlm_gpu_apply_host": [_vp, _vp, _vp],

@@ -336,11 +336,12 @@ __global__ void __launch_bounds__(kBtsThreads, 1) bt_rows_staged_kernel(DevSecto
     }
     __syncthreads();
     for (int c = tid; c < Dd; c += kBtsThreads) {
-      const float4 xv = xs[c];
-      const float dg = static_cast<float>(diag_value(S, u, S.dmask[c], cuu, S.cnt_dd[c], wp));
+      const int d = gauge_string(G, c);  // table position c serves output string d
+      const float4 xv = xs[d];
+      const float dg = static_cast<float>(diag_value(S, u, S.dmask[d], cuu, S.cnt_dd[d], wp));
       float4 acc = make_float4(dg * xv.x, dg * xv.y, dg * xv.z, dg * xv.w);
       bts_hops<kXor>(acc, G, c, smem_raw, tab, a0, a1);
-      Y4[base + static_cast<int64_t>(c) * (kBtChains / 2)] = acc;
+      Y4[base + static_cast<int64_t>(d) * (kBtChains / 2)] = acc;
     }
     __syncthreads();
   }

@@ -128,6 +128,9 @@ int upload_plan(ftlm_sector* s) {
     if (e != cudaSuccess) return e;
     out->ent = ge;
     out->grp = reinterpret_cast<const int4*>(gg);
+    uint8_t* gp;
+    if ((e = upload(G.perm, &gp, &s->owned)) != cudaSuccess) return e;
+    out->perm = gp;
     out->nt = static_cast<int>(G.tab.size() / 2);
     out->phase = G.phase ? 1 : 0;
     out->xor_real = G.xor_real ? 1 : 0;
@@ -337,11 +340,13 @@ int ftlm_gpu_sector_down_table_gauge(const ftlm_sector* s, int* available, long 
   return FTLM_OK;
 }
 
-int ftlm_gpu_sector_down_table_form(const ftlm_sector* s, int* phase, double* pc_ps, int* xor_real) {
+int ftlm_gpu_sector_down_table_form(const ftlm_sector* s, int* phase, double* pc_ps, int* xor_real,
+                                    unsigned char* lane_perm) {
   if (!s || !phase) return fail(FTLM_ERR_INVALID, "null argument");
   const GaugeTable& G = s->plan.dn_g;
   *phase = (G.ok && G.phase) ? 1 : 0;
   if (xor_real) *xor_real = (G.ok && G.xor_real) ? 1 : 0;
+  if (lane_perm && G.ok) std::copy(G.perm.begin(), G.perm.end(), lane_perm);
   if (pc_ps) {
     pc_ps[0] = G.pc;
     pc_ps[1] = G.ps;

@@ -15,7 +15,11 @@ struct DevGauge {
   int phase;            // 1: table-section coefficients are real2[cls] * (pc, +-ps) (entry bits 30, 27)
   double pc, ps;
   int xor_real;         // 1: real-section coefficient = real2[0] with its high word ^ (entry & 0xFFFC0000)
+  const uint8_t* perm;  // [ngroups * 32]: lane L of group g serves string g*32 + perm[g*32 + L]
 };
+
+// The output string served by table position c (group c / 32, lane c % 32).
+__device__ __forceinline__ int gauge_string(const DevGauge& G, int c) { return (c & ~31) | G.perm[c]; }
 
 struct DevSector {
   int n;

@@ -230,9 +230,8 @@ __global__ void __launch_bounds__(kRowThreads, 1) hv_rows_gauge_kernel(DevSector
     const int cuu = S.cnt_uu[r];
     const uint4 w = S.wpl[r];
     const double2* xrow = x + r * S.Dd;
-    uint32_t gbits = 0;  // bit j: g(u, d) of this thread's element j (d = tid + j * kRowThreads)
     int saw_tiny = 0;
-    for (int c = tid, j = 0; c < Dd; c += kRowThreads, ++j) {
+    for (int c = tid; c < Dd; c += kRowThreads) {
       double2 v = xrow[c];
       v.x *= sx;  // the input is sx * x (sx = 1: unchanged)
       v.y *= sx;
@@ -240,22 +239,21 @@ __global__ void __launch_bounds__(kRowThreads, 1) hv_rows_gauge_kernel(DevSector
         saw_tiny |= (v.x != 0.0 || v.y != 0.0);
         v = make_double2(0.0, 0.0);
       }
-      if (gauge_sign(u, S.dmask[c])) {
-        v = make_double2(-v.x, -v.y);
-        gbits |= 1u << j;
-      }
+      if (gauge_sign(u, S.dmask[c])) v = make_double2(-v.x, -v.y);
       xs[c] = v;
     }
     if (saw_tiny) atomicOr(S.flags, 1);
     __syncthreads();
     double2* yrow = y + r * S.Dd;
-    for (int c = tid, j = 0; c < Dd; c += kRowThreads, ++j) {
-      const double2 xv = xs[c];
-      const double dg = diag_value(S, u, S.dmask[c], cuu, S.cnt_dd[c], w);
+    for (int c = tid; c < Dd; c += kRowThreads) {
+      const int d = gauge_string(G, c);  // table position c serves output string d
+      const uint32_t dm = S.dmask[d];
+      const double2 xv = xs[d];
+      const double dg = diag_value(S, u, dm, cuu, S.cnt_dd[d], w);
       double2 acc = make_double2(dg * xv.x, dg * xv.y);
       gauge_hops<kPhase, kXor>(acc, G, c, smem_raw, tab, a0, a1);
-      if ((gbits >> j) & 1u) acc = make_double2(-acc.x, -acc.y);
-      yrow[c] = acc;
+      if (gauge_sign(u, dm)) acc = make_double2(-acc.x, -acc.y);
+      yrow[d] = acc;
     }
     __syncthreads();
   }

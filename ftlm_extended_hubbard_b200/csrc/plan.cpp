@@ -256,6 +256,68 @@ void build_gauge_table(const SpinSpace& sp, const std::vector<MergedHop>& hops, 
         (cls[static_cast<size_t>(h)] < 2 ? lr[l] : lt[l]).push_back(e);
       }
     }
+    // Lane permutation of a full group: the rounds of a section are set by the worst quarter-warp,
+    // max(its longest lane, its busiest bank group), so move strings between quarters to balance the
+    // bank-group loads (local search over swaps, deterministic per group); lane L serves string
+    // g*32 + perm[L].  The last, partial group keeps the identity.
+    uint8_t perm[32];
+    for (int l = 0; l < 32; ++l) perm[l] = static_cast<uint8_t>(l);
+    if (g * 32 + 32 <= D) {
+      int dl[2][32], dgp[2][32][8];
+      for (int l = 0; l < 32; ++l)
+        for (int sct = 0; sct < 2; ++sct) {
+          const auto& lst = sct ? lt[l] : lr[l];
+          dl[sct][l] = static_cast<int>(lst.size());
+          for (int b = 0; b < 8; ++b) dgp[sct][l][b] = 0;
+          for (uint32_t e : lst) ++dgp[sct][l][(e >> 10) & 7u];
+        }
+      auto cost = [&](const uint8_t* pm) {
+        int tot = 0;
+        for (int sct = 0; sct < 2; ++sct) {
+          int dm = 0;
+          for (int q = 0; q < 4; ++q) {
+            int m = 0, gs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            for (int k = 0; k < 8; ++k) {
+              const int l = pm[q * 8 + k];
+              m = std::max(m, dl[sct][l]);
+              for (int b = 0; b < 8; ++b) gs[b] += dgp[sct][l][b];
+            }
+            for (int b = 0; b < 8; ++b) m = std::max(m, gs[b]);
+            dm = std::max(dm, m);
+          }
+          tot += dm;
+        }
+        return tot;
+      };
+      uint64_t st64 = 0x9E3779B97F4A7C15ull ^ static_cast<uint64_t>(g);
+      auto rnd = [&st64]() {  // splitmix64
+        uint64_t z = (st64 += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+      };
+      int best = cost(perm);
+      for (int it = 0; it < 1500; ++it) {
+        const int a = static_cast<int>(rnd() % 32), b = static_cast<int>(rnd() % 32);
+        if (a / 8 == b / 8) continue;
+        std::swap(perm[a], perm[b]);
+        const int c = cost(perm);
+        if (c <= best)
+          best = c;
+        else
+          std::swap(perm[a], perm[b]);
+      }
+      std::vector<std::vector<uint32_t>> tr(32), tt(32);
+      for (int l = 0; l < 32; ++l) {
+        tr[l].swap(lr[perm[l]]);
+        tt[l].swap(lt[perm[l]]);
+      }
+      for (int l = 0; l < 32; ++l) {
+        lr[l].swap(tr[l]);
+        lt[l].swap(tt[l]);
+      }
+    }
+    for (int l = 0; l < 32; ++l) G.perm.push_back(perm[l]);
     size_t KR = 0, KT = 0;
     for (int qw = 0; qw < 4; ++qw) {
       schedule_quarter(&lr[8 * qw], &sr[8 * qw], pad_hop, D);

@@ -85,6 +85,10 @@ struct GaugeTable {
   std::vector<double> tab;
   std::vector<int32_t> grp;
   std::vector<uint32_t> ent;
+  // lane permutation, 32 per group: the entries of lane L of group g belong to output string
+  // g*32 + perm[32g + L] (the bank-group loads of the quarter-warps balanced; identity on the last,
+  // partial group)
+  std::vector<uint8_t> perm;
 };
 
 struct SectorPlan {

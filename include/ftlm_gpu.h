@@ -112,9 +112,12 @@ int ftlm_gpu_sector_down_table_gauge(const ftlm_sector* s, int* available, long 
  * (pc, ps); *phase = 0: the row pass loads table[t] (entry bits 18..26).  *xor_real = 1: a
  * real-section entry's bits 18..31 are the bits by which the high word of its signed coefficient
  * (-1)^s real2[cls] differs from that of real2[0] (same low word); *xor_real = 0: cls<<30 | s<<31.
- * Each section (KR, KT rounds) is padded to a multiple of 4 rounds.  Outputs other than phase may
- * be NULL. */
-int ftlm_gpu_sector_down_table_form(const ftlm_sector* s, int* phase, double* pc_ps, int* xor_real);
+ * Each section (KR, KT rounds) is padded to a multiple of 4 rounds.  lane_perm (n_groups * 32 bytes):
+ * lane L of group g holds the entries of output string g*32 + lane_perm[g*32 + L] (strings are
+ * moved between quarter-warps to balance their bank-group loads; the last, partial group is in
+ * order).  Outputs other than phase may be NULL. */
+int ftlm_gpu_sector_down_table_form(const ftlm_sector* s, int* phase, double* pc_ps, int* xor_real,
+                                    unsigned char* lane_perm);
 /* Host copy of the packed up-hop list of the column pass (inspection and tests; no reference
  * counterpart): *available = 0 when the sector has none (Du > 16384, more than 32 sites, or a
  * coefficient outside the form below; the column pass then reads the CSR list).  ptr: Du + 1

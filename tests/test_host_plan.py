@@ -211,7 +211,13 @@ def test_gauge_down_table_reproduces_oracle_row(c):
     assert tab is not None
     grp, ent, table, real2 = tab
     phase, pcps, xor = C.c_int(), np.zeros(2), C.c_int()
-    _lib.call("ftlm_gpu_sector_down_table_form", h, C.byref(phase), pcps.ctypes.data_as(C.c_void_p), C.byref(xor))
+    perm = np.zeros(32 * len(grp), np.uint8)
+    _lib.call("ftlm_gpu_sector_down_table_form", h, C.byref(phase), pcps.ctypes.data_as(C.c_void_p), C.byref(xor),
+              perm.ctypes.data_as(C.c_void_p))
+    perm = perm.reshape(-1, 32).astype(np.int64)
+    # lane L of group g serves string 32 g + perm[g, L]: a permutation of the group, the identity on a
+    # partial last group
+    assert all(sorted(row.tolist()) == list(range(32)) for row in perm)
     # one Peierls phase (phi_y == 0, or phi_x == 0) gives the phase form; two phases need the table
     assert phase.value == (1 if (px == 0.0) != (py == 0.0) else 0)
     # the XOR form needs the two real values to share their low words (t' = -0.25: -1 and 2 * 0.25)
@@ -222,6 +228,8 @@ def test_gauge_down_table_reproduces_oracle_row(c):
     up, dn = o.masks()
     Dd = int(np.count_nonzero(up == up[0]))
     assert len(grp) == (Dd + 31) // 32
+    if Dd % 32:
+        assert np.array_equal(perm[-1], np.arange(32))
     pps = np.array([_prefix_parity_shifted(int(d)) for d in dn[:Dd]], dtype=np.int64)
     rng = np.random.default_rng(5)
     for r in (0, (o.dim // Dd) // 2, o.dim // Dd - 1):
@@ -247,7 +255,7 @@ def test_gauge_down_table_reproduces_oracle_row(c):
                 for row in src[:, 8 * qw: 8 * qw + 8]:
                     assert len(set((row % 8).tolist())) == 8
             for l in range(32):
-                col = 32 * gi + l
+                col = 32 * gi + int(perm[gi, l])
                 if col >= Dd:
                     assert np.all(src[:, l] >= Dd)
                     continue
